@@ -1,0 +1,351 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 Walk-on-Spheres hot path (one JSON line on rank 0).
+
+Workload (one "step"): plain WoS, Poisson -Lap u = f with the manufactured
+solution u = sin(w x) sin(w y) sin(w z), w = 2 pi * 1.5, f = 3 w^2 u, Dirichlet
+g = u, on the seeded displaced icosphere (subdivision 6, 81,920 triangles,
+4-octave value noise, amplitude 0.12, base frequency 3, persistence 0.5,
+normalised to unit radius).  Evaluation points: the z = 0.12 slice, 512 x 512
+grid masked to the interior (GPU ray parity), 1,024 walks per point,
+epsilon = 5e-4, 256-step cap, FP32 walkers, FP64 per-point sums, in-ball
+Green's-function source sampling.  MSE is against the FP64 analytic u.
+
+value      = walk-steps (ball moves) of all ranks / max-over-ranks device time
+e2e        = same metric through the C ABI with host buffers: pinned H2D of the
+             points and D2H of the per-point FP64 sums inside the timed region
+roofline   = walker kernel: algorithmic bytes (node fetches x 128 B + triangle
+             tests x 48 B + point I/O) / kernel time, against the measured HBM
+             copy bandwidth (the BVH working set is L2-resident; see traffic)
+cpu_baseline = the oracle's scalar WoS port (same walk, CPU BVH) on the host
+             cores, bounded sample of the same workload
+
+--impl reference runs the reference path's CPU implementation (the oracle port
+of nc_wos_from_point over a CPU BVH; the reference's own walker exists only as
+GPU code built on cuBQL, which is not vendored) on rank 0 and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "n2wos-cuda_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "walk-steps/s (plain WoS, Poisson sin-product, icosphere L6, z=0.12 slice 512x512 x 1024 walks)"
+UNIT = "walk-steps/s"
+CONFIG = {
+    "workload": "plain WoS Poisson manufactured solution on displaced icosphere L6 (81,920 tris), "
+                "z=0.12 slice 512x512 masked to interior, 1024 walks/point, eps=5e-4, max_steps=256",
+    "mesh": "icosphere_displaced(level=6, amp=0.12, freq=3, octaves=4, persistence=0.5, seed=12345)",
+    "slice": {"view": "xy", "plane": 0.12, "width": 512, "height": 512, "padding": 0.02},
+    "walks_per_point": 1024, "epsilon": 5e-4, "max_steps": 256, "omega": "3*pi",
+    "source_sampling": "ball", "l2": "flushed between timed steps (256 MiB memset)",
+}
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+def peaks():
+    if MEASURED_PEAKS.exists():
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="n2w_clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path.exists():
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_scene(n2w, lib, call):
+    mesh = n2w.Mesh.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345)
+    mesh.normalize()
+    bvh = n2w.Bvh(mesh, 4, "sah")
+    lo, hi = mesh.bounds()
+    grid, frame = n2w.slice_points(lo, hi, "xy", 0.12, 512, 512, 0.02, True)
+    inside = bvh.inside(grid).astype(bool)
+    pts = np.ascontiguousarray(grid[inside])
+    problem = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
+    exact = n2w.problem_exact(problem, pts.astype(np.float64))
+    return mesh, bvh, pts, problem, exact, frame
+
+
+def cpu_port_sample(n2w, bvh_or_layout, problem, pts, walks, seconds_target=12.0, threads=None):
+    """Times the oracle's scalar WoS port on a bounded prefix of the points."""
+    import oracle
+
+    nodes, tris = bvh_or_layout
+    threads = threads or os.cpu_count() or 1
+    # calibration on a few points, then a sample sized for ~seconds_target
+    t0 = time.perf_counter()
+    r = oracle.wos(nodes, tris, bytes(problem), pts[:threads], walks, 256, 5e-4, 0.999, 12345, 0, threads)
+    dt = time.perf_counter() - t0
+    per_point = max(dt, 1e-6) / max(1, min(threads, len(pts)))
+    n = int(np.clip(seconds_target / per_point * threads, threads, len(pts)))
+    sel = pts[np.linspace(0, len(pts) - 1, n).astype(np.int64)]
+    t0 = time.perf_counter()
+    r = oracle.wos(nodes, tris, bytes(problem), sel, walks, 256, 5e-4, 0.999, 12345, 0, threads)
+    dt = time.perf_counter() - t0
+    steps = float(r["steps"].sum())
+    return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} of {len(pts)} slice points x {walks} walks ({steps:.3g} walk-steps) in {dt:.1f} s"}
+
+
+def run_reference(args):
+    import n2w
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from n2w._lib import call, lib  # noqa: F401 (host-only use: mesh, host BVH layout)
+
+    mesh = n2w.Mesh.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345)
+    mesh.normalize()
+    host = n2w.HostBvh(mesh, 4, "sah")
+    layout = host.layout()
+    lo, hi = mesh.bounds()
+    grid, _ = n2w.slice_points(lo, hi, "xy", 0.12, 512, 512, 0.02, True)
+    import oracle
+
+    v, t = mesh.arrays()
+    # interior mask with the reference rule on a strided subset (CPU brute force is O(points x tris))
+    cand = grid[::97]
+    inside = oracle.inside_bruteforce(v, t, cand).astype(bool)
+    pts = np.ascontiguousarray(cand[inside])
+    problem = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_port_sample(n2w, layout, problem, pts, 1024, seconds_target=8.0)
+        if i >= args.warmup:
+            vals.append(s)
+    value = float(np.mean([s["value"] for s in vals]))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[-1]["cores"], "kind": "port",
+                             "sample": vals[-1]["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference walker is GPU-only (cuBQL, not vendored); CPU path = oracle port of "
+                    "nc_wos_from_point (src/cuda/cubql_bvh.cu:1323-1357) over a CPU BVH, all host threads"}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="n2w", choices=["n2w", "reference"])
+    ap.add_argument("--walks", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import n2w
+    from n2w._lib import call, lib
+
+    call("n2w_set_device", local)
+    mesh, bvh, pts, problem, exact, frame = build_scene(n2w, lib, call)
+    n = len(pts)
+    W = args.walks
+    stream = n2w.Stream()
+    d_pts = n2w.DeviceBuffer.from_array(pts)
+    stats = n2w.PointStatsBuffers.allocate(n)
+    d_cnt = n2w.DeviceBuffer(C.sizeof(n2w._lib.WalkCounters))
+    d_ws = n2w.DeviceBuffer(lib.n2w_wos_workspace_bytes())
+    flush = n2w.DeviceBuffer(256 << 20)
+    opts = n2w.walk_options(walks_per_point=W, max_steps=256, epsilon=5e-4, step_scale=0.999,
+                            seed=12345 + 1000003 * rank)
+    timer = n2w.Timer()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def step(o):
+        call("n2w_wos_estimate", bvh.handle, C.byref(problem), d_pts.ptr, n, C.byref(o), stats.struct(),
+             d_cnt.ptr, d_ws.ptr, stream.handle)
+
+    for i in range(args.warmup):
+        step(opts)
+        stream.sync()
+
+    times, counters = [], []
+    with ClockSampler(local) as clocks:
+        barrier()
+        call("n2w_device_sync")
+        for i in range(args.steps):
+            flush.zero(stream)
+            timer.start(stream)
+            step(opts)
+            timer.stop(stream)
+            times.append(timer.ms())
+            raw = d_cnt.download(np.uint64, 8, stream)
+            counters.append(dict(zip([f for f, _ in n2w._lib.WalkCounters._fields_], map(int, raw))))
+        call("n2w_device_sync")
+        barrier()
+    total_ms = float(np.sum(times))
+    steps_done = float(sum(c["steps"] for c in counters))
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([total_ms, steps_done], dtype=torch.float64, device=f"cuda:{local}")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms, steps_done = float(tmax[0]), float(t[1])
+    value = steps_done / (total_ms / 1e3)
+
+    # accuracy of the last step (per-point FP64 sums -> MSE vs FP64 analytic)
+    res = stats.download(stream)
+    err = res["mean"] - exact
+    mse = float(np.mean(err ** 2))
+    var_part = float(np.mean(res["stderr"] ** 2))
+    bias2 = max(mse - var_part, 0.0)
+
+    # end to end: pinned host points in, per-point sums out, every step
+    hp = C.c_void_p()
+    call("n2w_malloc_host", C.byref(hp), pts.nbytes)
+    C.memmove(hp, pts.ctypes.data, pts.nbytes)
+    hout = C.c_void_p()
+    out_bytes = n * (8 + 8 + 4)
+    call("n2w_malloc_host", C.byref(hout), out_bytes)
+    e2e_times = []
+    barrier()
+    for i in range(max(1, args.steps)):
+        flush.zero(stream)
+        timer.start(stream)
+        call("n2w_memcpy_h2d", d_pts.ptr, hp, pts.nbytes, stream.handle)
+        step(opts)
+        call("n2w_memcpy_d2h", hout, stats.sum.ptr, 8 * n, stream.handle)
+        call("n2w_memcpy_d2h", C.c_void_p(hout.value + 8 * n), stats.sum_sq.ptr, 8 * n, stream.handle)
+        call("n2w_memcpy_d2h", C.c_void_p(hout.value + 16 * n), stats.count.ptr, 4 * n, stream.handle)
+        timer.stop(stream)
+        e2e_times.append(timer.ms())
+    barrier()
+    e2e_ms = float(np.sum(e2e_times))
+    e2e_steps = float(np.mean([c["steps"] for c in counters])) * len(e2e_times)
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([e2e_ms, e2e_steps], dtype=torch.float64, device=f"cuda:{local}")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        e2e_ms, e2e_steps = float(tmax[0]), float(t[1])
+    lib.n2w_free_host(hp)
+    lib.n2w_free_host(hout)
+
+    c_last = counters[-1]
+    kernel_ms = float(np.mean(times))
+    alg_bytes = c_last["node_visits"] * 128.0 + c_last["tri_tests"] * 48.0 + n * (12 + 8 + 8 + 4 + 8 + 4)
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                cpu = cpu_port_sample(n2w, bvh.layout(), problem, pts, W)
+            except Exception as e:  # the baseline must never break the bench line
+                cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                       "sample": f"failed: {e}"}
+        wsteps_per_walk = c_last["steps"] / max(c_last["walks"], 1)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(CONFIG, points=n, parallelism=f"replicas x{world} (distinct seeds)"),
+            "e2e": {"value": e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
+                    "d2h_bytes_per_step": int(out_bytes)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "walker_kernel", "bytes_per_launch": alg_bytes,
+                         "kernel_ms": kernel_ms},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "accuracy": {"mse_vs_fp64_exact": mse, "mean_estimator_variance": var_part, "bias2_estimate": bias2,
+                         "walks_per_point": W, "mean_steps_per_walk": wsteps_per_walk},
+            "time_to_mse_1e-4_s_plain_wos_extrapolated": (kernel_ms / 1e3) * var_part / max(1e-4 - bias2, 1e-12)
+            if bias2 < 1e-4 else None,
+            "counters_last_step": c_last,
+            "walks_per_s": c_last["walks"] / (kernel_ms / 1e3),
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

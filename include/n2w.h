@@ -1,0 +1,324 @@
+/*
+ * n2w.h — C ABI of the B200-native Walk-on-Spheres engine (libn2w.so).
+ *
+ * Plain C types only: pointers, sizes, POD structs.  Every function returns an
+ * int status (N2W_OK == 0) and records a human-readable message retrievable with
+ * n2w_last_error() on the calling thread.  Device pointers (d_*) are CUDA
+ * device addresses owned by the caller unless stated otherwise.  Stream
+ * arguments are cudaStream_t values passed as n2w_stream_t (NULL = legacy
+ * default stream).
+ *
+ * Reference interfaces replaced (paths inside Somatic-Cell/n2wos-cuda):
+ *   mesh generators / loaders / normalize  include/n2wos/mesh.hpp:9-19
+ *   CPU brute force closest point           include/n2wos/closest_point.hpp:9-17
+ *   CudaBvh / CuBqlBvh ctor + query_device  include/n2wos/cuda_bvh.hpp:34-57,
+ *                                           include/n2wos/cubql_bvh.hpp:33-65
+ *   NC walker launchers                     include/n2wos/tcnn_nc_wos.hpp:79-134
+ *   persistent WoS + reductions             src/cuda/cubql_bvh.cu:263-393,819-960
+ */
+#ifndef N2W_H_
+#define N2W_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define N2W_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define N2W_OK 0
+#define N2W_EINVAL 1    /* invalid argument (null pointer, bad size, bad mode) */
+#define N2W_ECUDA 2     /* CUDA runtime error (message holds cudaGetErrorString) */
+#define N2W_ENOMEM 3    /* host or device allocation failed / admission refused */
+#define N2W_ETIMEOUT 4  /* a device-side budget or deadline expired */
+#define N2W_EIO 5       /* file could not be read or parsed */
+#define N2W_EINTERNAL 6 /* internal invariant violated */
+
+typedef struct CUstream_st* n2w_stream_t; /* == cudaStream_t */
+
+/* 12-byte AoS point, layout-identical to the reference's DeviceVec3
+ * (src/cuda/bvh_types.cuh:17-21). */
+typedef struct n2w_vec3 {
+  float x, y, z;
+} n2w_vec3;
+
+typedef struct n2w_mesh n2w_mesh; /* host triangle mesh (opaque) */
+typedef struct n2w_bvh n2w_bvh;   /* device-resident BVH + triangles (opaque) */
+
+const char* n2w_last_error(void);
+int n2w_abi_version(void);
+/* Fills buf with "runtime=<v>,driver=<v>" (reference cuda_bvh.hpp:79). */
+int n2w_cuda_runtime_version_string(char* buf, size_t cap);
+/* Fills buf with "<name> sm_<maj><min> global_mem=<bytes>" (reference cuda_bvh.hpp:80). */
+int n2w_cuda_device_summary(char* buf, size_t cap);
+
+/* ---- meshes (host) ------------------------------------------------------ */
+/* Copies nv vertices (xyz float triples) and nt triangles (uint32 triples). */
+int n2w_mesh_create(const float* vertices, int64_t nv, const uint32_t* triangles, int64_t nt,
+                    const char* name, n2w_mesh** out);
+/* Reference bumpy-sphere surface (src/mesh/procedural_bumpy_sphere.cpp:12-90). */
+int n2w_mesh_bumpy_sphere_ref(int stacks, int slices, float amplitude, n2w_mesh** out);
+/* Same UV topology, radius r = 1 + amplitude*sin(k_theta*theta)*cos(k_phi*phi). */
+int n2w_mesh_bumpy_sphere_trig(int stacks, int slices, float amplitude, int k_theta, int k_phi,
+                               n2w_mesh** out);
+/* Subdivided icosahedron (20*4^level triangles) radially displaced by seeded
+ * multi-octave value noise: r = 1 + amplitude * noise(x). */
+int n2w_mesh_icosphere_displaced(int level, float amplitude, float base_frequency, int octaves,
+                                 float persistence, uint64_t seed, n2w_mesh** out);
+int n2w_mesh_load_ply(const char* path, n2w_mesh** out);
+int n2w_mesh_load_obj(const char* path, n2w_mesh** out);
+/* AABB-centre translate + scale by max vertex radius (reference src/mesh/normalize.cpp:18-37).
+ * center_out[3] and scale_out (=1/radius) may be NULL. */
+int n2w_mesh_normalize(n2w_mesh* mesh, float* center_out, float* scale_out);
+int n2w_mesh_counts(const n2w_mesh* mesh, int64_t* nv, int64_t* nt);
+/* Copies vertices (3*nv floats) and triangles (3*nt uint32); either may be NULL. */
+int n2w_mesh_copy_out(const n2w_mesh* mesh, float* vertices, uint32_t* triangles);
+/* bounds_out[6] = min xyz, max xyz. */
+int n2w_mesh_bounds(const n2w_mesh* mesh, float* bounds_out);
+/* Number of triangles with |cross(b-a,c-a)|^2 <= area2_epsilon (reference closest_point.cpp:70-83). */
+int n2w_mesh_count_degenerate(const n2w_mesh* mesh, float area2_epsilon, int64_t* out);
+void n2w_mesh_free(n2w_mesh* mesh);
+
+/* ---- BVH + closest point ----------------------------------------------- */
+typedef struct n2w_bvh_stats {
+  int64_t triangles;      /* triangles stored (= mesh triangles) */
+  int64_t nodes;          /* 4-wide nodes on the device */
+  int64_t binary_nodes;   /* nodes of the binary tree before collapsing */
+  int64_t leaves;         /* leaf references */
+  int32_t leaf_size;      /* maximum triangles per leaf */
+  int32_t max_depth;      /* depth of the 4-wide tree (root = 0) */
+  double build_milliseconds; /* host build + upload wall time */
+  double sah_cost;        /* SAH cost of the binary tree (traversal 1, intersection 1) */
+  int64_t device_bytes;   /* bytes resident on the device */
+} n2w_bvh_stats;
+
+/* Host-only build of the same layout (no device needed): nodes (128 B each)
+ * and leaf-ordered triangles (48 B each) for inspection and CPU restatements. */
+typedef struct n2w_bvh_host n2w_bvh_host;
+int n2w_bvh_host_build(const n2w_mesh* mesh, int leaf_size, const char* build_method,
+                       n2w_bvh_host** out);
+int n2w_bvh_host_stats(const n2w_bvh_host* h, n2w_bvh_stats* out);
+int n2w_bvh_host_copy(const n2w_bvh_host* h, void* nodes_out, void* tris_out);
+void n2w_bvh_host_free(n2w_bvh_host* h);
+
+/* Builds on the host and uploads to the current device.  build_method:
+ * "sah" (binned SAH, default when NULL) or "spatial_median" (largest-centroid-axis
+ * median split, the reference's in-tree builder, bvh_build_host.cpp:74-120).
+ * leaf_size in [1, 8]. */
+int n2w_bvh_create(const n2w_mesh* mesh, int leaf_size, const char* build_method, n2w_bvh** out);
+int n2w_bvh_stats_get(const n2w_bvh* bvh, n2w_bvh_stats* out);
+void n2w_bvh_destroy(n2w_bvh* bvh);
+
+/* Exact closest point on the mesh for each query point (reference
+ * CudaBvh::query_device, include/n2wos/cuda_bvh.hpp:50-57; cubql_bvh.hpp:45-52).
+ * Outputs: squared distance, closest point, triangle index (lowest index on exact
+ * distance ties, identical to the CPU brute force), stack-overflow flag.
+ * query_count == 0 is a no-op; < 0 or null pointers -> N2W_EINVAL;
+ * block_size outside [1,1024] -> N2W_EINVAL.  No allocation, no host transfer. */
+int n2w_bvh_query_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
+                         float* d_distance2, n2w_vec3* d_closest, int* d_triangle_id,
+                         int* d_overflow, int block_size, n2w_stream_t stream);
+/* Masked variant (reference cubql_bvh.hpp:57-65): slots with d_active[i]==0 skip
+ * traversal and write d2=0, closest=query point, tri=-1, overflow=0. */
+int n2w_bvh_query_device_masked(const n2w_bvh* bvh, const n2w_vec3* d_points,
+                                const uint8_t* d_active, int query_count, float* d_distance2,
+                                n2w_vec3* d_closest, int* d_triangle_id, int* d_overflow,
+                                int block_size, n2w_stream_t stream);
+/* Diagnostic variant: also writes per-query node visits and triangle tests
+ * (d_node_visits / d_tri_tests, int32 each) for algorithmic-byte accounting. */
+int n2w_bvh_query_device_counted(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
+                                 float* d_distance2, n2w_vec3* d_closest, int* d_triangle_id,
+                                 int* d_overflow, int* d_node_visits, int* d_tri_tests,
+                                 int block_size, n2w_stream_t stream);
+/* Inside/outside classification of a closed mesh by +x ray parity, with the
+ * reference's ray test and query offset (src/cuda/cubql_bvh.cu:407-455, which
+ * runs it on the CPU for slice masks).  d_inside[i] = 1 inside, 0 outside;
+ * *d_overflow (device int, caller-zeroed) is set to 1 if a stack overflowed. */
+int n2w_bvh_inside_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
+                          uint8_t* d_inside, int* d_overflow, int block_size, n2w_stream_t stream);
+/* Slice grid of the reference renderer (src/cuda/cubql_bvh.cu:963-1025): view
+ * "xy"|"xz"|"yz", frame from the mesh bounds grown by padding_fraction, widened
+ * to the pixel aspect when preserve_aspect; pixel (ix, iy) -> points[iy*W+ix].
+ * frame_out[4] = u_min, u_max, v_min, v_max (may be NULL). */
+int n2w_slice_points(const float* bounds6, const char* view, float plane, int width, int height,
+                     float padding_fraction, int preserve_aspect, float* points_out, float* frame_out);
+/* Copies the device layout back to the host: nodes (128 B each) and leaf-ordered
+ * triangles (48 B each).  Either pointer may be NULL.  Used by the CPU restatement
+ * of the traversal to count visits. */
+int n2w_bvh_copy_layout(const n2w_bvh* bvh, void* nodes_out, void* tris_out);
+
+/* ---- boundary value problems ------------------------------------------- */
+/* Boundary / source modes.  Values 0..16 and 30..32 keep the reference's
+ * NcBoundaryMode ids (include/n2wos/tcnn_nc_wos.hpp:14-35); 100+ are new. */
+#define N2W_BC_HARMONIC_X2_MINUS_Y2 0
+#define N2W_BC_EXTERNAL_CHARGES_MEDIUM 1
+#define N2W_BC_EXTERNAL_CHARGES_HIGH 2
+#define N2W_BC_HARMONIC_ZEBRA_K4 3
+#define N2W_BC_HARMONIC_ZEBRA_K8 4
+#define N2W_BC_HARMONIC_ZEBRA_K12 5
+#define N2W_BC_EXTERNAL_CHARGES_SHELL_K8 6
+#define N2W_BC_EXTERNAL_CHARGES_SHELL_K16 7
+#define N2W_BC_TEXTURE_STRIPES_K8 8
+#define N2W_BC_TEXTURE_STRIPES_K16 9
+#define N2W_BC_TEXTURE_CHECKER_K8 10
+#define N2W_BC_TEXTURE_CHECKER_K16 11
+#define N2W_BC_CONSTANT_ONE 12
+#define N2W_BC_POISSON_MULTISCALE 30
+#define N2W_BC_POISSON_FIGLIKE_HF 31
+#define N2W_BC_CHARGES_SEEDED 100   /* sum_k a_k / |x - c_k| with a seeded charge set */
+#define N2W_BC_POISSON_SINPROD 101  /* u = sin(w x) sin(w y) sin(w z), f = 3 w^2 u */
+
+#define N2W_SOURCE_BALL 0    /* source sampled inside each ball from its Green's function */
+#define N2W_SOURCE_CENTER 1  /* reference rule r^2/6 * f(ball centre), exact for harmonic f */
+
+#define N2W_MAX_CHARGES 16
+
+typedef struct n2w_problem {
+  int32_t mode;             /* N2W_BC_* */
+  int32_t source_sampling;  /* N2W_SOURCE_* (ignored for harmonic problems) */
+  int32_t charge_count;     /* for N2W_BC_CHARGES_SEEDED */
+  float omega;              /* for N2W_BC_POISSON_SINPROD */
+  float charges[N2W_MAX_CHARGES][4]; /* x, y, z, amplitude */
+} n2w_problem;
+
+/* Seeded charge set: centres uniform in the spherical shell r in [r_min, r_max]
+ * (uniform in volume), amplitudes uniform in [-1, 1]; stream = splitmix64(seed). */
+int n2w_problem_charges_seeded(int count, float r_min, float r_max, uint64_t seed,
+                               n2w_problem* out);
+int n2w_problem_sinprod(float omega, int source_sampling, n2w_problem* out);
+int n2w_problem_reference_mode(int mode, int source_sampling, n2w_problem* out);
+/* Exact solution u(x) (FP64 where analytic) for n points (host arrays). */
+int n2w_problem_exact(const n2w_problem* problem, const double* xyz, int64_t n, double* u_out);
+/* Dirichlet data g and source f as the device evaluates them (FP32), host side. */
+int n2w_problem_eval_f32(const n2w_problem* problem, const float* xyz, int64_t n, float* g_out,
+                         float* f_out);
+/* Case-insensitive name -> mode id (reference parse_nc_boundary_mode aliases,
+ * src/cuda/cubql_bvh.cu:1739-1800, plus "charges_seeded", "poisson_sinprod"). */
+int n2w_problem_mode_from_name(const char* name, int* mode_out);
+const char* n2w_problem_mode_name(int mode);
+
+/* ---- walkers ------------------------------------------------------------ */
+#define N2W_WALK_PURE 0      /* walk to the epsilon shell */
+#define N2W_WALK_PREFIX 1    /* stop at depth_m, emit X_m for the cache (coarse level) */
+#define N2W_WALK_RESIDUAL 2  /* record X_m at depth_m, continue to the boundary */
+
+typedef struct n2w_walk_options {
+  int32_t walks_per_point;
+  int32_t max_steps;     /* reference default 256 */
+  int32_t depth_m;       /* truncation depth for PREFIX / RESIDUAL */
+  float epsilon;         /* stopping shell width */
+  float step_scale;      /* ball radius = step_scale * distance (reference 0.999) */
+  uint64_t seed;         /* Philox key */
+  int32_t block_size;    /* threads per block of the persistent walker (0 = tuned default) */
+  int32_t blocks_per_sm; /* resident blocks per SM (0 = occupancy maximum) */
+  int32_t chunk;         /* walks a lane takes per queue pop (0 = tuned default) */
+  int32_t accumulate;    /* 0: outputs are overwritten; 1: results are added */
+  int64_t deadline_ns;   /* 0 = none; else walkers stop this many ns after launch */
+} n2w_walk_options;
+
+/* Per-point FP64 estimator accumulators (device arrays, one entry per point). */
+typedef struct n2w_point_stats {
+  double* d_sum;          /* sum of sample values */
+  double* d_sum_sq;       /* sum of squared sample values */
+  uint32_t* d_count;      /* samples accumulated */
+  uint64_t* d_steps;      /* sum of walk steps (ball moves) */
+  uint32_t* d_forced;     /* walks stopped by max_steps */
+} n2w_point_stats;
+
+/* Run-level counters written by the walker (device struct, zeroed by the call). */
+typedef struct n2w_walk_counters {
+  unsigned long long walks;        /* walks finished */
+  unsigned long long steps;        /* ball moves (walk-steps) */
+  unsigned long long queries;      /* closest-point queries */
+  unsigned long long node_visits;  /* 4-wide node fetches */
+  unsigned long long tri_tests;    /* triangle tests */
+  unsigned long long overflow;     /* traversal stack overflows */
+  unsigned long long forced;       /* walks stopped by max_steps */
+  unsigned long long timed_out;    /* walks abandoned by the deadline */
+} n2w_walk_counters;
+
+/* Host evaluation of the walkers' generator: Philox4x32-10 of counter ctr[4]
+ * under the key the walkers derive from (seed, tag); tag 0 = plain walks,
+ * 1 = coarse (PREFIX) walks, 2 = residual walks.  Lets a caller reproduce the
+ * random numbers of walk w = point*W + j at step s: ctr = {w, w>>32, s, 0|1}. */
+int n2w_rng_philox4x32_10(const uint32_t* ctr, uint64_t seed, uint32_t tag, uint32_t* out);
+
+/* Workspace bytes the walker needs (work-queue counter + counters). */
+size_t n2w_wos_workspace_bytes(void);
+
+/* Plain WoS estimate of u at each point with per-point FP64 reductions on the
+ * device: persistent walker, counter-based Philox RNG, queue regeneration.
+ * d_workspace may be NULL (then stream-ordered memory is taken from the CUDA
+ * pool for the call).  d_counters (device) may be NULL. */
+int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
+                     int64_t point_count, const n2w_walk_options* options,
+                     n2w_point_stats stats, n2w_walk_counters* d_counters, void* d_workspace,
+                     n2w_stream_t stream);
+
+/* Per-sample outputs, mirroring launch_nc_pure_wos_samples
+ * (include/n2wos/tcnn_nc_wos.hpp:87-93): sample j of point i is at i*W+j. */
+int n2w_wos_pure_samples(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
+                         int64_t point_count, const n2w_walk_options* options,
+                         float* d_sample_values, int* d_step_count, int* d_forced_max_steps,
+                         int* d_query_overflow, n2w_stream_t stream);
+
+/* Coarse (PREFIX) and residual (RESIDUAL) walks for NC / 2LMC, mirroring
+ * launch_nc_hybrid_prefix and launch_nc_2lmc_prefix_continue
+ * (include/n2wos/tcnn_nc_wos.hpp:95-124).  Per sample: X_m mapped to the unit
+ * cube by (x - input_min) / input_extent (reference cubql_bvh.cu:1311-1315),
+ * the prefix value A_m (source accumulated to depth m, plus boundary value if
+ * the walk stopped earlier), needs_cache flag, and for RESIDUAL the value of the
+ * continuation (A_m + continuation).  d_continuation_values may be NULL for PREFIX. */
+int n2w_wos_prefix_samples(const n2w_bvh* bvh, const n2w_problem* problem,
+                           const n2w_vec3* d_points, int64_t point_count,
+                           const n2w_walk_options* options, int mode, const float* input_min,
+                           const float* input_extent, float* d_prefix_inputs,
+                           float* d_boundary_values, float* d_continuation_values,
+                           uint8_t* d_needs_cache, int* d_step_count, int* d_forced_max_steps,
+                           int* d_query_overflow, n2w_stream_t stream);
+
+/* nc = A + C*needs, residual = needs ? W - C : 0 (reference cubql_bvh.cu:1608-1627). */
+int n2w_wos_combine(const float* d_cache_outputs, const float* d_boundary_values,
+                    const float* d_continuation_values, const uint8_t* d_needs_cache,
+                    int64_t sample_count, float* d_nc_values, float* d_residual_values,
+                    int block_size, n2w_stream_t stream);
+
+/* Per-point FP64 reduction of per-sample arrays (sample j of point i at i*W+j):
+ * warp shuffles + FP64 atomics (replaces the host summaries of
+ * src/tools/eval_tcnn_nc_wos.cu:525-569). */
+int n2w_reduce_samples(const float* d_values, const int* d_step_count, const int* d_forced,
+                       int64_t point_count, int walks_per_point, n2w_point_stats stats,
+                       int accumulate, n2w_stream_t stream);
+
+/* ---- thin device-memory helpers for callers without a CUDA binding ------ */
+int n2w_device_count(int* out);
+int n2w_set_device(int device);
+int n2w_malloc(void** d_ptr, size_t bytes);
+int n2w_free(void* d_ptr);
+int n2w_malloc_host(void** h_ptr, size_t bytes); /* pinned */
+int n2w_free_host(void* h_ptr);
+int n2w_memcpy_h2d(void* d_dst, const void* h_src, size_t bytes, n2w_stream_t stream);
+int n2w_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, n2w_stream_t stream);
+int n2w_memset(void* d_ptr, int value, size_t bytes, n2w_stream_t stream);
+int n2w_stream_create(n2w_stream_t* out);
+int n2w_stream_destroy(n2w_stream_t stream);
+int n2w_stream_sync(n2w_stream_t stream);
+int n2w_device_sync(void);
+/* Records a pair of events around nothing: timer handle for callers. */
+typedef struct n2w_timer n2w_timer;
+int n2w_timer_create(n2w_timer** out);
+int n2w_timer_start(n2w_timer* t, n2w_stream_t stream);
+int n2w_timer_stop(n2w_timer* t, n2w_stream_t stream);
+int n2w_timer_elapsed_ms(n2w_timer* t, float* ms_out); /* synchronises on the stop event */
+void n2w_timer_destroy(n2w_timer* t);
+int n2w_sm_count(int* out);
+int n2w_mem_info(size_t* free_bytes, size_t* total_bytes);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* N2W_H_ */

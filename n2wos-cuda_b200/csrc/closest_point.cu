@@ -1,0 +1,224 @@
+// Device-pointer closest-point queries over the 4-wide BVH (reference
+// CudaBvh::query_device, src/cuda/bvh_query.cu:228-261, and the masked cuBQL
+// variant, src/cuda/cubql_bvh.cu:187-214).  One thread per query, ordered
+// traversal with the stack in per-thread local memory (geom.cuh).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+
+#include "geom.cuh"
+#include "internal.hpp"
+
+namespace n2w {
+namespace {
+
+template <bool kMasked, bool kCount>
+__global__ void __launch_bounds__(256) closest_point_kernel(
+    const float4* __restrict__ nodes, const float4* __restrict__ tris,
+    const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
+    float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
+    int* __restrict__ out_overflow, int* __restrict__ out_nodes, int* __restrict__ out_tris) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const n2w_vec3 pt = points[q];
+  if (kMasked && active[q] == 0) {
+    out_d2[q] = 0.0f;
+    out_cp[q] = pt;
+    out_id[q] = -1;
+    out_overflow[q] = 0;
+    if (kCount) {
+      out_nodes[q] = 0;
+      out_tris[q] = 0;
+    }
+    return;
+  }
+  dev::ClosestHit hit;
+  hit.d2 = FLT_MAX;
+  hit.id = INT32_MAX;
+  hit.cp = dev::v3(0.0f, 0.0f, 0.0f);
+  dev::TraversalStats st{0, 0, 0};
+  dev::traverse<kCount>(nodes, tris, dev::v3(pt.x, pt.y, pt.z), hit, st);
+  out_d2[q] = hit.d2;
+  out_cp[q] = n2w_vec3{hit.cp.x, hit.cp.y, hit.cp.z};
+  out_id[q] = hit.id == INT32_MAX ? -1 : hit.id;
+  out_overflow[q] = st.overflow;
+  if (kCount) {
+    out_nodes[q] = st.node_visits;
+    out_tris[q] = st.tri_tests;
+  }
+}
+
+// Inside/outside by ray parity along +x with the reference's deterministic
+// offset (src/cuda/cubql_bvh.cu:446-455).
+__global__ void __launch_bounds__(256) inside_kernel(const float4* __restrict__ nodes,
+                                                     const float4* __restrict__ tris,
+                                                     const n2w_vec3* __restrict__ points, int n,
+                                                     uint8_t* __restrict__ inside, int* __restrict__ overflow) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const n2w_vec3 p = points[q];
+  int ov = 0;
+  const int hits = dev::ray_x_crossings(nodes, tris, dev::v3(p.x, p.y + 1.928371e-6f, p.z + 3.141593e-6f), ov);
+  inside[q] = (hits & 1) ? 1 : 0;
+  if (ov) atomicOr(overflow, 1);
+}
+
+}  // namespace
+
+void launch_inside(const n2w_bvh& bvh, const n2w_vec3* d_points, int n, uint8_t* d_inside, int* d_overflow,
+                   int block_size, cudaStream_t stream) {
+  const int grid = (n + block_size - 1) / block_size;
+  inside_kernel<<<grid, block_size, 0, stream>>>(reinterpret_cast<const float4*>(bvh.d_nodes),
+                                                 reinterpret_cast<const float4*>(bvh.d_tris), d_points, n,
+                                                 d_inside, d_overflow);
+  N2W_CUDA(cudaGetLastError());
+}
+
+void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const uint8_t* d_active,
+                          int n, float* d_d2, n2w_vec3* d_cp, int* d_id, int* d_overflow,
+                          int* d_nodes, int* d_tris, int block_size, cudaStream_t stream) {
+  const int grid = (n + block_size - 1) / block_size;
+  const float4* nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
+  const float4* tris = reinterpret_cast<const float4*>(bvh.d_tris);
+  if (d_nodes) {
+    closest_point_kernel<false, true><<<grid, block_size, 0, stream>>>(
+        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, d_nodes, d_tris);
+  } else if (d_active) {
+    closest_point_kernel<true, false><<<grid, block_size, 0, stream>>>(
+        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
+  } else {
+    closest_point_kernel<false, false><<<grid, block_size, 0, stream>>>(
+        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
+  }
+  N2W_CUDA(cudaGetLastError());
+}
+
+int sm_count_current() {
+  int dev = 0, sms = 0;
+  N2W_CUDA(cudaGetDevice(&dev));
+  N2W_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return sms;
+}
+
+}  // namespace n2w
+
+using namespace n2w;
+
+namespace {
+
+void check_query_args(const n2w_bvh* bvh, const void* pts, int n, const void* d2, const void* cp,
+                      const void* id, const void* ov, int block_size) {
+  N2W_REQUIRE(bvh && bvh->d_nodes && bvh->d_tris, "query_device called on empty BVH");
+  N2W_REQUIRE(n >= 0, "query_device query_count must be non-negative");
+  if (n == 0) return;
+  N2W_REQUIRE(pts && d2 && cp && id && ov, "query_device received a null device pointer");
+  N2W_REQUIRE(block_size >= 1 && block_size <= 1024, "CUDA block size must be in [1, 1024]");
+}
+
+}  // namespace
+
+extern "C" {
+
+int n2w_bvh_create(const n2w_mesh* mesh, int leaf_size, const char* build_method, n2w_bvh** out) {
+  return guarded([&] {
+    N2W_REQUIRE(mesh && out, "n2w_bvh_create: null argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    HostBvh h = build_bvh4(*mesh, leaf_size, build_method ? build_method : "sah");
+    auto* b = new n2w_bvh();
+    try {
+      N2W_CUDA(cudaGetDevice(&b->device));
+      N2W_CUDA(cudaMalloc(&b->d_nodes, h.nodes.size() * sizeof(Node4)));
+      N2W_CUDA(cudaMalloc(&b->d_tris, h.tris.size() * sizeof(TriRec)));
+      N2W_CUDA(cudaMemcpy(b->d_nodes, h.nodes.data(), h.nodes.size() * sizeof(Node4), cudaMemcpyHostToDevice));
+      N2W_CUDA(cudaMemcpy(b->d_tris, h.tris.data(), h.tris.size() * sizeof(TriRec), cudaMemcpyHostToDevice));
+    } catch (...) {
+      if (b->d_nodes) cudaFree(b->d_nodes);
+      if (b->d_tris) cudaFree(b->d_tris);
+      delete b;
+      throw;
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    b->stats = host_stats(h, leaf_size, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    *out = b;
+  });
+}
+
+int n2w_bvh_stats_get(const n2w_bvh* bvh, n2w_bvh_stats* out) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && out, "null argument");
+    *out = bvh->stats;
+  });
+}
+
+void n2w_bvh_destroy(n2w_bvh* bvh) {
+  if (!bvh) return;
+  if (bvh->d_nodes) cudaFree(bvh->d_nodes);
+  if (bvh->d_tris) cudaFree(bvh->d_tris);
+  delete bvh;
+}
+
+int n2w_bvh_query_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
+                         float* d_distance2, n2w_vec3* d_closest, int* d_triangle_id,
+                         int* d_overflow, int block_size, n2w_stream_t stream) {
+  return guarded([&] {
+    check_query_args(bvh, d_points, query_count, d_distance2, d_closest, d_triangle_id, d_overflow, block_size);
+    if (query_count == 0) return;
+    launch_closest_point(*bvh, d_points, nullptr, query_count, d_distance2, d_closest, d_triangle_id,
+                         d_overflow, nullptr, nullptr, block_size, stream);
+  });
+}
+
+int n2w_bvh_query_device_masked(const n2w_bvh* bvh, const n2w_vec3* d_points,
+                                const uint8_t* d_active, int query_count, float* d_distance2,
+                                n2w_vec3* d_closest, int* d_triangle_id, int* d_overflow,
+                                int block_size, n2w_stream_t stream) {
+  return guarded([&] {
+    check_query_args(bvh, d_points, query_count, d_distance2, d_closest, d_triangle_id, d_overflow, block_size);
+    if (query_count == 0) return;
+    N2W_REQUIRE(d_active, "query_device_masked received a null mask");
+    launch_closest_point(*bvh, d_points, d_active, query_count, d_distance2, d_closest, d_triangle_id,
+                         d_overflow, nullptr, nullptr, block_size, stream);
+  });
+}
+
+int n2w_bvh_query_device_counted(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
+                                 float* d_distance2, n2w_vec3* d_closest, int* d_triangle_id,
+                                 int* d_overflow, int* d_node_visits, int* d_tri_tests,
+                                 int block_size, n2w_stream_t stream) {
+  return guarded([&] {
+    check_query_args(bvh, d_points, query_count, d_distance2, d_closest, d_triangle_id, d_overflow, block_size);
+    if (query_count == 0) return;
+    N2W_REQUIRE(d_node_visits && d_tri_tests, "counted query needs counter outputs");
+    launch_closest_point(*bvh, d_points, nullptr, query_count, d_distance2, d_closest, d_triangle_id,
+                         d_overflow, d_node_visits, d_tri_tests, block_size, stream);
+  });
+}
+
+int n2w_bvh_inside_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count, uint8_t* d_inside,
+                          int* d_overflow, int block_size, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && bvh->d_nodes && bvh->d_tris, "inside_device called on empty BVH");
+    N2W_REQUIRE(query_count >= 0, "query_count must be non-negative");
+    if (query_count == 0) return;
+    N2W_REQUIRE(d_points && d_inside && d_overflow, "inside_device received a null device pointer");
+    N2W_REQUIRE(block_size >= 1 && block_size <= 1024, "CUDA block size must be in [1, 1024]");
+    launch_inside(*bvh, d_points, query_count, d_inside, d_overflow, block_size, stream);
+  });
+}
+
+int n2w_bvh_copy_layout(const n2w_bvh* bvh, void* nodes_out, void* tris_out) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh, "null bvh");
+    if (nodes_out) {
+      N2W_CUDA(cudaMemcpy(nodes_out, bvh->d_nodes, static_cast<size_t>(bvh->stats.nodes) * sizeof(Node4),
+                          cudaMemcpyDeviceToHost));
+    }
+    if (tris_out) {
+      N2W_CUDA(cudaMemcpy(tris_out, bvh->d_tris, static_cast<size_t>(bvh->stats.triangles) * sizeof(TriRec),
+                          cudaMemcpyDeviceToHost));
+    }
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,271 @@
+// Exact point-triangle closest point and the 4-wide BVH traversal (device).
+//
+// The triangle routine restates Ericson, Real-Time Collision Detection §5.1.5,
+// in the operation order of the reference CPU oracle
+// (src/geometry/closest_point.cpp:7-48, device twin src/cuda/bvh_query.cu:33-73).
+// Every arithmetic step uses a round-to-nearest intrinsic (__fadd_rn etc.), which
+// the compiler never fuses into an FMA, so results are bit-identical to the
+// reference's g++ build of the same expressions.  The box distance uses the
+// same non-fused operations, which keeps it a rounding-monotone lower bound of
+// every contained triangle's computed distance: pruning with `box_d2 > best_d2`
+// therefore never drops a triangle whose distance ties the current best, and the
+// (d2, id) tie-break returns the lowest triangle id among exact ties — the
+// answer of the reference brute force, which keeps the first minimum in index
+// order (closest_point.cpp:57-65).
+#pragma once
+
+#include <float.h>
+#include <stdint.h>
+
+#include "layout.h"
+
+namespace n2w {
+namespace dev {
+
+struct V3 {
+  float x, y, z;
+};
+
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 vsub(V3 a, V3 b) { return V3{fs(a.x, b.x), fs(a.y, b.y), fs(a.z, b.z)}; }
+__device__ __forceinline__ V3 vadd(V3 a, V3 b) { return V3{fa(a.x, b.x), fa(a.y, b.y), fa(a.z, b.z)}; }
+__device__ __forceinline__ V3 vscale(V3 a, float s) { return V3{fm(a.x, s), fm(a.y, s), fm(a.z, s)}; }
+__device__ __forceinline__ float vdot(V3 a, V3 b) { return fa(fa(fm(a.x, b.x), fm(a.y, b.y)), fm(a.z, b.z)); }
+
+// Ericson closest point on triangle abc to p, reference operation order.
+__device__ __forceinline__ V3 closest_point_triangle(V3 p, V3 a, V3 b, V3 c) {
+  const V3 ab = vsub(b, a);
+  const V3 ac = vsub(c, a);
+  const V3 ap = vsub(p, a);
+  const float d1 = vdot(ab, ap);
+  const float d2 = vdot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) return a;
+
+  const V3 bp = vsub(p, b);
+  const float d3 = vdot(ab, bp);
+  const float d4 = vdot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) return b;
+
+  const float vc = fs(fm(d1, d4), fm(d3, d2));
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+    const float v = fd(d1, fs(d1, d3));
+    return vadd(a, vscale(ab, v));
+  }
+
+  const V3 cp = vsub(p, c);
+  const float d5 = vdot(ab, cp);
+  const float d6 = vdot(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) return c;
+
+  const float vb = fs(fm(d5, d2), fm(d1, d6));
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+    const float w = fd(d2, fs(d2, d6));
+    return vadd(a, vscale(ac, w));
+  }
+
+  const float va = fs(fm(d3, d6), fm(d5, d4));
+  const float d43 = fs(d4, d3);
+  const float d56 = fs(d5, d6);
+  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) {
+    const float w = fd(d43, fa(d43, d56));
+    return vadd(b, vscale(vsub(c, b), w));
+  }
+
+  const float denom = fd(1.0f, fa(fa(va, vb), vc));
+  const float v = fm(vb, denom);
+  const float w = fm(vc, denom);
+  return vadd(vadd(a, vscale(ab, v)), vscale(ac, w));
+}
+
+// Squared distance from p to box [lo, hi] along one axis pair; +inf for empty slots.
+__device__ __forceinline__ float axis_gap(float p, float lo, float hi) {
+  return fmaxf(fmaxf(fs(lo, p), fs(p, hi)), 0.0f);
+}
+
+__device__ __forceinline__ float box_d2(V3 p, float lox, float hix, float loy, float hiy, float loz,
+                                        float hiz) {
+  const float dx = axis_gap(p.x, lox, hix);
+  const float dy = axis_gap(p.y, loy, hiy);
+  const float dz = axis_gap(p.z, loz, hiz);
+  return fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz));
+}
+
+__device__ __forceinline__ void cswap(float& da, int& ra, float& db, int& rb) {
+  if (db < da) {
+    const float td = da;
+    da = db;
+    db = td;
+    const int tr = ra;
+    ra = rb;
+    rb = tr;
+  }
+}
+
+struct ClosestHit {
+  float d2;
+  int id;  // original triangle id; INT32_MAX when nothing was found below the bound
+  V3 cp;
+};
+
+struct TraversalStats {
+  int node_visits;
+  int tri_tests;
+  int overflow;
+};
+
+// Ordered depth-first traversal: at each inner node the four child boxes are
+// measured, sorted ascending (fixed 5-comparator network), the nearest child
+// is entered and the others are pushed far-to-near.  Popped entries are
+// re-checked against the current best.  Candidates are any triangles whose box
+// distance is <= best_d2; `hit` must be initialised by the caller (cold query:
+// d2 = FLT_MAX, id = INT32_MAX; warm start: d2 = an upper bound).
+template <bool kCount>
+__device__ __forceinline__ void traverse(const float4* __restrict__ nodes,
+                                         const float4* __restrict__ tris, V3 p, ClosestHit& hit,
+                                         TraversalStats& st) {
+  int2 stack[kTraversalStack];
+  int sp = 0;
+  int32_t ref = 0;
+  for (;;) {
+    if (ref >= 0) {
+      const float4* n = nodes + static_cast<size_t>(ref) * 8;
+      const float4 lox = __ldg(n + 0);
+      const float4 hix = __ldg(n + 1);
+      const float4 loy = __ldg(n + 2);
+      const float4 hiy = __ldg(n + 3);
+      const float4 loz = __ldg(n + 4);
+      const float4 hiz = __ldg(n + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
+      if (kCount) ++st.node_visits;
+      float d0 = box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
+      float d1 = box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
+      float d2 = box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
+      float d3 = box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
+      int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
+      cswap(d0, r0, d1, r1);
+      cswap(d2, r2, d3, r3);
+      cswap(d0, r0, d2, r2);
+      cswap(d1, r1, d3, r3);
+      cswap(d1, r1, d2, r2);
+      const float best = hit.d2;
+      if (d3 <= best) {
+        if (sp < kTraversalStack) stack[sp++] = make_int2(r3, __float_as_int(d3));
+        else st.overflow = 1;
+      }
+      if (d2 <= best) {
+        if (sp < kTraversalStack) stack[sp++] = make_int2(r2, __float_as_int(d2));
+        else st.overflow = 1;
+      }
+      if (d1 <= best) {
+        if (sp < kTraversalStack) stack[sp++] = make_int2(r1, __float_as_int(d1));
+        else st.overflow = 1;
+      }
+      ref = (d0 <= best) ? r0 : kEmptyChild;
+    } else if (ref != kEmptyChild) {
+      const int first = leaf_first(ref);
+      const int count = leaf_count(ref);
+      const float4* t = tris + static_cast<size_t>(first) * 3;
+      for (int i = 0; i < count; ++i) {
+        const float4 a = __ldg(t + 3 * i + 0);
+        const float4 b = __ldg(t + 3 * i + 1);
+        const float4 c = __ldg(t + 3 * i + 2);
+        if (kCount) ++st.tri_tests;
+        const V3 cp = closest_point_triangle(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z));
+        const V3 dv = vsub(cp, p);
+        const float dd = vdot(dv, dv);
+        const int id = __float_as_int(a.w);
+        if (dd < hit.d2 || (dd == hit.d2 && id < hit.id)) {
+          hit.d2 = dd;
+          hit.id = id;
+          hit.cp = cp;
+        }
+      }
+      ref = kEmptyChild;
+    }
+    if (ref == kEmptyChild) {
+      bool found = false;
+      while (sp > 0) {
+        const int2 e = stack[--sp];
+        if (__int_as_float(e.y) <= hit.d2) {
+          ref = e.x;
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+  }
+}
+
+// +x ray / triangle test of the reference's slice mask
+// (src/cuda/cubql_bvh.cu:407-428, Möller–Trumbore with its tolerances), in the
+// same non-fused float operations, so the parity count matches the CPU test.
+__device__ __forceinline__ bool ray_x_hits(V3 p, V3 a, V3 b, V3 c) {
+  const float y_min = fminf(fminf(a.y, b.y), c.y), y_max = fmaxf(fmaxf(a.y, b.y), c.y);
+  const float z_min = fminf(fminf(a.z, b.z), c.z), z_max = fmaxf(fmaxf(a.z, b.z), c.z);
+  const float x_max = fmaxf(fmaxf(a.x, b.x), c.x);
+  if (p.y < y_min || p.y > y_max || p.z < z_min || p.z > z_max || p.x > x_max) return false;
+  const V3 e1 = vsub(b, a);
+  const V3 e2 = vsub(c, a);
+  // h = cross((1,0,0), e2)
+  const V3 h = v3(fs(fm(0.0f, e2.z), fm(0.0f, e2.y)), fs(fm(0.0f, e2.x), fm(1.0f, e2.z)),
+                  fs(fm(1.0f, e2.y), fm(0.0f, e2.x)));
+  const float det = vdot(e1, h);
+  if (fabsf(det) < 1.0e-12f) return false;
+  const float inv_det = fd(1.0f, det);
+  const V3 s = vsub(p, a);
+  const float u = fm(inv_det, vdot(s, h));
+  if (u < -1.0e-7f || u > 1.0f + 1.0e-7f) return false;
+  const V3 q = v3(fs(fm(s.y, e1.z), fm(s.z, e1.y)), fs(fm(s.z, e1.x), fm(s.x, e1.z)),
+                  fs(fm(s.x, e1.y), fm(s.y, e1.x)));
+  const float v = fm(inv_det, vdot(v3(1.0f, 0.0f, 0.0f), q));
+  if (v < -1.0e-7f || fa(u, v) > 1.0f + 1.0e-7f) return false;
+  const float t = fm(inv_det, vdot(e2, q));
+  return t > 1.0e-7f;
+}
+
+// Number of mesh triangles crossed by the +x ray from p (every node whose
+// child box meets the ray {x >= p.x, y = p.y, z = p.z} is visited).
+__device__ __forceinline__ int ray_x_crossings(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                               V3 p, int& overflow) {
+  int stack[kTraversalStack];
+  int sp = 0;
+  int hits = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const int ref = stack[--sp];
+    if (ref >= 0) {
+      const float4* n = nodes + static_cast<size_t>(ref) * 8;
+      const float4 hix = __ldg(n + 1), loy = __ldg(n + 2), hiy = __ldg(n + 3), loz = __ldg(n + 4),
+                   hiz = __ldg(n + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
+      const float hx[4] = {hix.x, hix.y, hix.z, hix.w}, ly[4] = {loy.x, loy.y, loy.z, loy.w},
+                  hy[4] = {hiy.x, hiy.y, hiy.z, hiy.w}, lz[4] = {loz.x, loz.y, loz.z, loz.w},
+                  hz[4] = {hiz.x, hiz.y, hiz.z, hiz.w};
+      const int cr[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (cr[k] == kEmptyChild) continue;
+        if (p.y < ly[k] || p.y > hy[k] || p.z < lz[k] || p.z > hz[k] || p.x > hx[k]) continue;
+        if (sp < kTraversalStack) stack[sp++] = cr[k];
+        else overflow = 1;
+      }
+    } else {
+      const int first = leaf_first(ref), count = leaf_count(ref);
+      const float4* t = tris + static_cast<size_t>(first) * 3;
+      for (int i = 0; i < count; ++i) {
+        const float4 a = __ldg(t + 3 * i), b = __ldg(t + 3 * i + 1), c = __ldg(t + 3 * i + 2);
+        if (ray_x_hits(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z))) ++hits;
+      }
+    }
+  }
+  return hits;
+}
+
+}  // namespace dev
+}  // namespace n2w

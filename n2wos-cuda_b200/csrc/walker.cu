@@ -1,0 +1,592 @@
+// Persistent Walk-on-Spheres walkers with on-device estimator reductions.
+//
+// Semantics follow the reference walk (src/cuda/cubql_bvh.cu:1323-1357,
+// 263-336): for step = 0..max_steps query the closest point P at x, d = |x-P|;
+// stop if d <= epsilon, step >= max_steps or d is not finite and score g(P);
+// otherwise add the ball's source contribution, move x += step_scale*d*dir with
+// dir uniform on the unit sphere (z = 1-2u, phi = 2 pi v, reference 254-261).
+//
+// B200 design:
+//  * a grid of SMs x resident blocks that lives until the work runs out; each
+//    lane owns one walker and pops `chunk` consecutive walks of one point from
+//    a global queue with one warp-aggregated atomic, so uneven walk lengths
+//    never idle a lane while work remains;
+//  * counter-based Philox keyed by (seed; walk id, step, stream), so a walk's
+//    path is independent of scheduling (serving "alone == in the mix");
+//  * every query after the first is warm-started with the squared distance to
+//    the previous closest point (an upper bound of the new distance), which
+//    prunes the BVH to the walker's neighbourhood without changing the result;
+//  * per-point FP64 sum / sum of squares accumulated per lane over its chunk,
+//    merged across lanes with warp shuffles and flushed with FP64 atomics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "geom.cuh"
+#include "internal.hpp"
+#include "philox.cuh"
+#include "problem.cuh"
+#include "walker.cuh"
+
+namespace n2w {
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ dev::V3 unit_sphere(uint32_t a, uint32_t b) {
+  const float z = 1.0f - 2.0f * u01(a);
+  float s, c;
+  sincospif(2.0f * u01(b), &s, &c);
+  const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  return dev::v3(r * c, r * s, z);
+}
+
+// Beta(2,2) inverse CDF: the radius fraction t of a point drawn from the ball's
+// Green's function density G(x,y) ∝ 1/|y-x| - 1/R (radial density ∝ t(1-t)).
+// Solves 3t^2 - 2t^3 = u with the trigonometric root of the depressed cubic.
+__device__ __forceinline__ float green_radius_fraction(float u) {
+  const float a = acosf(fminf(1.0f, fmaxf(-1.0f, 1.0f - 2.0f * u)));
+  return 0.5f + cosf((a - 6.283185307179586f) * (1.0f / 3.0f));
+}
+
+__device__ __forceinline__ double shfl_xor_d(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+
+// Warp-collective flush of per-lane chunk accumulators into per-point FP64
+// totals: lanes are grouped by point id, each group is reduced by a shuffle
+// butterfly (non-members contribute zero) and its lowest lane issues the atomics.
+__device__ __forceinline__ void warp_flush(bool want, int64_t pid, double s, double s2, uint32_t n,
+                                           uint64_t steps, uint32_t forced, const WalkArgs& a) {
+  unsigned pending = __ballot_sync(0xffffffffu, want);
+  const int lane = threadIdx.x & 31;
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const long long lp = __shfl_sync(0xffffffffu, static_cast<long long>(pid), leader);
+    const bool in = want && pid == lp;
+    const unsigned grp = __ballot_sync(0xffffffffu, in);
+    double vs = in ? s : 0.0, vs2 = in ? s2 : 0.0;
+    unsigned long long vst = in ? steps : 0ull;
+    unsigned vn = in ? n : 0u, vf = in ? forced : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vs += shfl_xor_d(vs, o);
+      vs2 += shfl_xor_d(vs2, o);
+      vst += __shfl_xor_sync(0xffffffffu, vst, o);
+      vn += __shfl_xor_sync(0xffffffffu, vn, o);
+      vf += __shfl_xor_sync(0xffffffffu, vf, o);
+    }
+    if (lane == leader) {
+      atomicAdd(a.sum + lp, vs);
+      atomicAdd(a.sum_sq + lp, vs2);
+      atomicAdd(a.count + lp, vn);
+      atomicAdd(reinterpret_cast<unsigned long long*>(a.steps) + lp, vst);
+      atomicAdd(a.forced + lp, vf);
+    }
+    pending &= ~grp;
+  }
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int kOut, int kWalk>
+__global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArgs a) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t t_start = (a.deadline_ns > 0) ? global_ns() : 0;
+
+  bool alive = false;     // a walk is in progress on this lane
+  bool exhausted = false; // the global queue has no chunk left for this lane
+  int64_t pid = -1;
+  int walk = 0, walk_end = 0;
+  dev::V3 x = dev::v3(0, 0, 0), P = dev::v3(0, 0, 0), xm = dev::v3(0, 0, 0);
+  float src = 0.0f, am = 0.0f;
+  int step = 0, cont0 = 0;
+  bool has_xm = false;
+  uint64_t wid = 0;
+
+  double acc_s = 0.0, acc_s2 = 0.0;
+  uint32_t acc_n = 0, acc_forced = 0;
+  uint64_t acc_steps = 0;
+
+  unsigned long long c_walks = 0, c_steps = 0, c_queries = 0, c_nodes = 0, c_tris = 0, c_overflow = 0,
+                     c_forced = 0, c_timeout = 0;
+
+  for (;;) {
+    // (1) deadline: abandon the current walk and stop taking work.
+    if (a.deadline_ns > 0 && !exhausted && (global_ns() - t_start) > static_cast<uint64_t>(a.deadline_ns)) {
+      if (alive) ++c_timeout;
+      alive = false;
+      exhausted = true;
+      walk = walk_end;
+    }
+    // (2) flush a finished (or abandoned) chunk's accumulators; always before
+    //     the exit test below, so nothing accumulated is ever dropped.
+    if (kOut == kOutStats) {
+      const bool want = !alive && walk >= walk_end && acc_n > 0;
+      warp_flush(want, pid, acc_s, acc_s2, acc_n, acc_steps, acc_forced, a);
+      if (want) {
+        acc_s = acc_s2 = 0.0;
+        acc_n = acc_forced = 0;
+        acc_steps = 0;
+      }
+    }
+    // (3) next walk of the current chunk, else pop a new chunk.
+    bool start = false;
+    if (!alive && !exhausted && walk < walk_end) start = true;
+    const bool need = !alive && !exhausted && !start;
+    const unsigned need_mask = __ballot_sync(0xffffffffu, need);
+    if (need_mask) {
+      const int leader = __ffs(need_mask) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(a.queue, static_cast<unsigned long long>(__popc(need_mask)));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const unsigned long long c = base + __popc(need_mask & ((1u << lane) - 1u));
+        if (c < static_cast<unsigned long long>(a.total_chunks)) {
+          pid = static_cast<int64_t>(c / static_cast<unsigned long long>(a.chunks_per_point));
+          walk = static_cast<int>((c % static_cast<unsigned long long>(a.chunks_per_point)) * a.chunk);
+          walk_end = min(walk + a.chunk, a.walks_per_point);
+          start = true;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (start) {
+      const n2w_vec3 p0 = a.points[pid];
+      x = dev::v3(p0.x, p0.y, p0.z);
+      src = 0.0f;
+      step = 0;
+      cont0 = 0;
+      has_xm = false;
+      wid = static_cast<uint64_t>(pid) * static_cast<uint64_t>(a.walks_per_point) + static_cast<uint64_t>(walk);
+      alive = true;
+    }
+    if (!__any_sync(0xffffffffu, alive)) break;
+    if (!alive) continue;
+
+    // (4) one closest-point query + one ball move.
+    dev::ClosestHit hit;
+    hit.id = INT32_MAX;
+    hit.cp = x;
+    if (step == 0) {
+      hit.d2 = FLT_MAX;
+    } else {
+      const float dx = x.x - P.x, dy = x.y - P.y, dz = x.z - P.z;
+      const float db = sqrtf(dx * dx + dy * dy + dz * dz) * 1.0001f + 2.0e-6f;
+      hit.d2 = db * db;
+    }
+    dev::TraversalStats st{0, 0, 0};
+    dev::traverse<true>(a.nodes, a.tris, x, hit, st);
+    if (hit.id == INT32_MAX && step > 0) {
+      // The warm bound sat below the numerically computed minimum; redo cold.
+      hit.d2 = FLT_MAX;
+      hit.cp = x;
+      dev::traverse<true>(a.nodes, a.tris, x, hit, st);
+    }
+    ++c_queries;
+    c_nodes += st.node_visits;
+    c_tris += st.tri_tests;
+    c_overflow += st.overflow;
+
+    const float d = sqrtf(fmaxf(hit.d2, 0.0f));
+    const int rel = step - cont0;  // steps since the walk (or its continuation) began
+    const bool forced = rel >= a.max_steps;
+    const bool stop = d <= a.eps || forced || !isfinite(d) || hit.id == INT32_MAX;
+    bool finished = false;
+    float value = 0.0f;
+    if (stop) {
+      value = src + problem_u<float>(a.problem, hit.cp.x, hit.cp.y, hit.cp.z);
+      finished = true;
+    } else if (kWalk == N2W_WALK_PREFIX && step >= a.depth_m) {
+      value = src;
+      finished = true;
+    }
+    if (finished) {
+      ++c_walks;
+      c_steps += static_cast<unsigned long long>(step);
+      c_forced += forced ? 1ull : 0ull;
+      if (kOut == kOutStats) {
+        acc_s += static_cast<double>(value);
+        acc_s2 += static_cast<double>(value) * static_cast<double>(value);
+        ++acc_n;
+        acc_steps += static_cast<uint64_t>(step);
+        acc_forced += forced ? 1u : 0u;
+      } else {
+        const uint64_t s = wid;
+        if (kOut == kOutSamples) {
+          a.s_value[s] = value;
+          a.s_steps[s] = step;
+          a.s_forced[s] = forced ? 1 : 0;
+          a.s_overflow[s] = st.overflow;
+        } else {
+          // Prefix outputs (reference cubql_bvh.cu:1451-1606): X is X_m when the
+          // cache is needed, else the position where the walk stopped.
+          const bool needs = (kWalk == N2W_WALK_PREFIX) ? !stop : has_xm;
+          const dev::V3 xo = (kWalk == N2W_WALK_RESIDUAL && has_xm) ? xm : x;
+          a.p_inputs[3 * s + 0] = fminf(1.0f, fmaxf(0.0f, (xo.x - a.in_min[0]) / fmaxf(a.in_ext[0], 1.0e-6f)));
+          a.p_inputs[3 * s + 1] = fminf(1.0f, fmaxf(0.0f, (xo.y - a.in_min[1]) / fmaxf(a.in_ext[1], 1.0e-6f)));
+          a.p_inputs[3 * s + 2] = fminf(1.0f, fmaxf(0.0f, (xo.z - a.in_min[2]) / fmaxf(a.in_ext[2], 1.0e-6f)));
+          a.p_needs[s] = needs ? 1 : 0;
+          if (kWalk == N2W_WALK_PREFIX) {
+            a.p_boundary[s] = value;
+          } else {
+            a.p_boundary[s] = needs ? am : value;
+            a.p_cont[s] = needs ? (value - am) : value;
+          }
+          a.s_steps[s] = step;
+          a.s_forced[s] = forced ? 1 : 0;
+          a.s_overflow[s] = st.overflow;
+        }
+      }
+      alive = false;
+      ++walk;
+      continue;
+    }
+
+    if (kWalk == N2W_WALK_RESIDUAL && step == a.depth_m && !has_xm) {
+      // X_m reached: remember it and the prefix source; the continuation gets a
+      // fresh max_steps budget like the reference's nc_wos_from_point(X_m).
+      xm = x;
+      am = src;
+      has_xm = true;
+      cont0 = step;
+    }
+    const float R = a.step_scale * d;
+    const U4 r = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                  static_cast<uint32_t>(step), 0u},
+                               a.k0, a.k1);
+    const dev::V3 dir = unit_sphere(r.x, r.y);
+    if (a.has_source) {
+      float f;
+      if (a.source_center) {
+        f = problem_f<float>(a.problem, x.x, x.y, x.z);
+      } else {
+        const float t = green_radius_fraction(u01(r.z));
+        const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                       static_cast<uint32_t>(step), 1u},
+                                    a.k0, a.k1);
+        const dev::V3 w = unit_sphere(r2.x, r2.y);
+        const float rho = R * t;
+        f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
+      }
+      src += (R * R) * (1.0f / 6.0f) * f;
+    }
+    P = hit.cp;
+    x = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
+    ++step;
+  }
+
+  if (a.counters) {
+    c_walks = warp_sum_u64(c_walks);
+    c_steps = warp_sum_u64(c_steps);
+    c_queries = warp_sum_u64(c_queries);
+    c_nodes = warp_sum_u64(c_nodes);
+    c_tris = warp_sum_u64(c_tris);
+    c_overflow = warp_sum_u64(c_overflow);
+    c_forced = warp_sum_u64(c_forced);
+    c_timeout = warp_sum_u64(c_timeout);
+    if (lane == 0) {
+      atomicAdd(&a.counters->walks, c_walks);
+      atomicAdd(&a.counters->steps, c_steps);
+      atomicAdd(&a.counters->queries, c_queries);
+      atomicAdd(&a.counters->node_visits, c_nodes);
+      atomicAdd(&a.counters->tri_tests, c_tris);
+      atomicAdd(&a.counters->overflow, c_overflow);
+      atomicAdd(&a.counters->forced, c_forced);
+      atomicAdd(&a.counters->timed_out, c_timeout);
+    }
+  }
+}
+
+// ---- per-sample reduction and 2LMC combination ------------------------------
+__global__ void reduce_samples_kernel(const float* __restrict__ values, const int* __restrict__ steps,
+                                      const int* __restrict__ forced, int64_t points, int W,
+                                      double* sum, double* sum_sq, uint32_t* count, uint64_t* st,
+                                      uint32_t* fc) {
+  // One warp per (point, 32*k slice): lanes stride the point's samples, then a
+  // shuffle butterfly and one FP64 atomic per warp.
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps_per_point = (W + 1023) / 1024;
+  const int64_t pid = warp / warps_per_point;
+  if (pid >= points) return;
+  const int64_t part = warp % warps_per_point;
+  const int j0 = static_cast<int>(part * 1024);
+  const int j1 = min(W, j0 + 1024);
+  double s = 0.0, s2 = 0.0;
+  unsigned long long ns = 0;
+  unsigned n = 0, f = 0;
+  for (int j = j0 + lane; j < j1; j += 32) {
+    const int64_t k = pid * W + j;
+    const double v = values[k];
+    s += v;
+    s2 += v * v;
+    ++n;
+    if (steps) ns += static_cast<unsigned long long>(steps[k]);
+    if (forced) f += forced[k] ? 1u : 0u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += shfl_xor_d(s, o);
+    s2 += shfl_xor_d(s2, o);
+    ns += __shfl_xor_sync(0xffffffffu, ns, o);
+    n += __shfl_xor_sync(0xffffffffu, n, o);
+    f += __shfl_xor_sync(0xffffffffu, f, o);
+  }
+  if (lane == 0) {
+    atomicAdd(sum + pid, s);
+    atomicAdd(sum_sq + pid, s2);
+    atomicAdd(count + pid, n);
+    if (st) atomicAdd(reinterpret_cast<unsigned long long*>(st) + pid, ns);
+    if (fc) atomicAdd(fc + pid, f);
+  }
+}
+
+__global__ void combine_kernel(const float* __restrict__ cache, const float* __restrict__ boundary,
+                               const float* __restrict__ cont, const uint8_t* __restrict__ needs,
+                               int64_t n, float* __restrict__ nc, float* __restrict__ residual) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (needs[i]) {
+    const float c = cache[i];
+    nc[i] = boundary[i] + c;
+    residual[i] = cont[i] - c;
+  } else {
+    nc[i] = boundary[i];
+    residual[i] = 0.0f;
+  }
+}
+
+// ---- host side -----------------------------------------------------------
+namespace {
+
+template <int kOut, int kWalk>
+void launch_walker(const WalkArgs& a, int block, int blocks_per_sm, cudaStream_t stream) {
+  auto kern = walker_kernel<kOut, kWalk>;
+  int occ = 0;
+  N2W_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, 0));
+  if (occ < 1) occ = 1;
+  const int per_sm = blocks_per_sm > 0 ? std::min(blocks_per_sm, occ) : occ;
+  const int64_t lanes_needed = a.total_chunks;
+  int64_t grid = static_cast<int64_t>(sm_count_current()) * per_sm;
+  grid = std::min<int64_t>(grid, (lanes_needed + block - 1) / block);
+  grid = std::max<int64_t>(grid, 1);
+  kern<<<static_cast<unsigned>(grid), block, 0, stream>>>(a);
+  N2W_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void validate_walk_options(const n2w_walk_options& o) {
+  N2W_REQUIRE(o.walks_per_point > 0, "walks_per_point must be positive");
+  N2W_REQUIRE(o.max_steps > 0, "max_steps must be positive");
+  N2W_REQUIRE(o.depth_m >= 0, "depth_m must be non-negative");
+  N2W_REQUIRE(o.epsilon > 0.0f, "epsilon must be positive");
+  N2W_REQUIRE(o.step_scale > 0.0f && o.step_scale <= 1.0f, "step_scale must be in (0, 1]");
+  N2W_REQUIRE(o.block_size == 0 || (o.block_size >= 32 && o.block_size <= kWalkerMaxThreads && o.block_size % 32 == 0),
+              "walker block_size must be 0 or a multiple of 32 in [32, 256]");
+  N2W_REQUIRE(o.chunk >= 0, "chunk must be non-negative");
+  N2W_REQUIRE(o.blocks_per_sm >= 0, "blocks_per_sm must be non-negative");
+}
+
+void validate_problem(const n2w_problem& p) {
+  const int m = p.mode;
+  const bool ok = (m >= 0 && m <= 12) || m == N2W_BC_POISSON_MULTISCALE || m == N2W_BC_POISSON_FIGLIKE_HF ||
+                  m == N2W_BC_CHARGES_SEEDED || m == N2W_BC_POISSON_SINPROD;
+  N2W_REQUIRE(ok, "unsupported boundary mode " + std::to_string(m));
+  N2W_REQUIRE(p.source_sampling == N2W_SOURCE_BALL || p.source_sampling == N2W_SOURCE_CENTER,
+              "source_sampling must be N2W_SOURCE_BALL or N2W_SOURCE_CENTER");
+  if (m == N2W_BC_CHARGES_SEEDED) {
+    N2W_REQUIRE(p.charge_count >= 1 && p.charge_count <= N2W_MAX_CHARGES, "charge_count must be in [1, 16]");
+  }
+}
+
+WalkArgs make_walk_args(const n2w_bvh& bvh, const n2w_problem& problem, const n2w_vec3* d_points,
+                        int64_t point_count, const n2w_walk_options& o, uint32_t stream_tag) {
+  WalkArgs a{};
+  a.nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
+  a.tris = reinterpret_cast<const float4*>(bvh.d_tris);
+  a.points = d_points;
+  a.walks_per_point = o.walks_per_point;
+  a.chunk = o.chunk > 0 ? std::min(o.chunk, o.walks_per_point) : std::min(kDefaultChunk, o.walks_per_point);
+  a.chunks_per_point = (o.walks_per_point + a.chunk - 1) / a.chunk;
+  a.total_chunks = point_count * a.chunks_per_point;
+  a.max_steps = o.max_steps;
+  a.depth_m = o.depth_m;
+  a.eps = o.epsilon;
+  a.step_scale = o.step_scale;
+  philox_key(o.seed, stream_tag, a.k0, a.k1);
+  a.problem = problem;
+  a.has_source = problem_has_source(problem) ? 1 : 0;
+  a.source_center = problem.source_sampling == N2W_SOURCE_CENTER ? 1 : 0;
+  a.deadline_ns = o.deadline_ns;
+  return a;
+}
+
+void run_walker(WalkArgs& a, int out_kind, int walk_mode, const n2w_walk_options& o, n2w_walk_counters* d_counters,
+                void* d_workspace, cudaStream_t stream) {
+  if (a.total_chunks == 0) return;
+  void* ws = d_workspace;
+  bool own = false;
+  if (!ws) {
+    N2W_CUDA(cudaMallocAsync(&ws, n2w_wos_workspace_bytes(), stream));
+    own = true;
+  }
+  N2W_CUDA(cudaMemsetAsync(ws, 0, n2w_wos_workspace_bytes(), stream));
+  a.queue = reinterpret_cast<unsigned long long*>(ws);
+  a.counters = d_counters ? d_counters : reinterpret_cast<n2w_walk_counters*>(reinterpret_cast<char*>(ws) + 256);
+  if (d_counters) N2W_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(n2w_walk_counters), stream));
+  const int block = o.block_size > 0 ? o.block_size : kDefaultWalkerThreads;
+  if (out_kind == kOutStats) launch_walker<kOutStats, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
+  else if (out_kind == kOutSamples) launch_walker<kOutSamples, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
+  else if (walk_mode == N2W_WALK_PREFIX) launch_walker<kOutPrefix, N2W_WALK_PREFIX>(a, block, o.blocks_per_sm, stream);
+  else launch_walker<kOutPrefix, N2W_WALK_RESIDUAL>(a, block, o.blocks_per_sm, stream);
+  if (own) N2W_CUDA(cudaFreeAsync(ws, stream));
+}
+
+void zero_stats(const n2w_point_stats& s, int64_t n, cudaStream_t stream) {
+  N2W_CUDA(cudaMemsetAsync(s.d_sum, 0, sizeof(double) * n, stream));
+  N2W_CUDA(cudaMemsetAsync(s.d_sum_sq, 0, sizeof(double) * n, stream));
+  N2W_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(uint32_t) * n, stream));
+  N2W_CUDA(cudaMemsetAsync(s.d_steps, 0, sizeof(uint64_t) * n, stream));
+  N2W_CUDA(cudaMemsetAsync(s.d_forced, 0, sizeof(uint32_t) * n, stream));
+}
+
+}  // namespace n2w
+
+using namespace n2w;
+
+extern "C" {
+
+size_t n2w_wos_workspace_bytes(void) { return 512; }
+
+int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
+                     int64_t point_count, const n2w_walk_options* options, n2w_point_stats stats,
+                     n2w_walk_counters* d_counters, void* d_workspace, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && bvh->d_nodes && problem && options, "n2w_wos_estimate: null argument");
+    N2W_REQUIRE(point_count >= 0, "point_count must be non-negative");
+    validate_walk_options(*options);
+    validate_problem(*problem);
+    if (point_count == 0) return;
+    N2W_REQUIRE(d_points && stats.d_sum && stats.d_sum_sq && stats.d_count && stats.d_steps && stats.d_forced,
+                "n2w_wos_estimate: null device pointer");
+    if (!options->accumulate) zero_stats(stats, point_count, stream);
+    WalkArgs a = make_walk_args(*bvh, *problem, d_points, point_count, *options, 0);
+    a.sum = stats.d_sum;
+    a.sum_sq = stats.d_sum_sq;
+    a.count = stats.d_count;
+    a.steps = stats.d_steps;
+    a.forced = stats.d_forced;
+    run_walker(a, kOutStats, N2W_WALK_PURE, *options, d_counters, d_workspace, stream);
+  });
+}
+
+int n2w_wos_pure_samples(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
+                         int64_t point_count, const n2w_walk_options* options,
+                         float* d_sample_values, int* d_step_count, int* d_forced_max_steps,
+                         int* d_query_overflow, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && bvh->d_nodes && problem && options, "n2w_wos_pure_samples: null argument");
+    N2W_REQUIRE(point_count >= 0, "point_count must be non-negative");
+    validate_walk_options(*options);
+    validate_problem(*problem);
+    if (point_count == 0) return;
+    N2W_REQUIRE(d_points && d_sample_values && d_step_count && d_forced_max_steps && d_query_overflow,
+                "n2w_wos_pure_samples: null device pointer");
+    WalkArgs a = make_walk_args(*bvh, *problem, d_points, point_count, *options, 0);
+    a.s_value = d_sample_values;
+    a.s_steps = d_step_count;
+    a.s_forced = d_forced_max_steps;
+    a.s_overflow = d_query_overflow;
+    run_walker(a, kOutSamples, N2W_WALK_PURE, *options, nullptr, nullptr, stream);
+  });
+}
+
+int n2w_wos_prefix_samples(const n2w_bvh* bvh, const n2w_problem* problem,
+                           const n2w_vec3* d_points, int64_t point_count,
+                           const n2w_walk_options* options, int mode, const float* input_min,
+                           const float* input_extent, float* d_prefix_inputs,
+                           float* d_boundary_values, float* d_continuation_values,
+                           uint8_t* d_needs_cache, int* d_step_count, int* d_forced_max_steps,
+                           int* d_query_overflow, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && bvh->d_nodes && problem && options && input_min && input_extent,
+                "n2w_wos_prefix_samples: null argument");
+    N2W_REQUIRE(mode == N2W_WALK_PREFIX || mode == N2W_WALK_RESIDUAL, "mode must be PREFIX or RESIDUAL");
+    N2W_REQUIRE(point_count >= 0, "point_count must be non-negative");
+    validate_walk_options(*options);
+    validate_problem(*problem);
+    if (point_count == 0) return;
+    N2W_REQUIRE(d_points && d_prefix_inputs && d_boundary_values && d_needs_cache && d_step_count &&
+                    d_forced_max_steps && d_query_overflow,
+                "n2w_wos_prefix_samples: null device pointer");
+    N2W_REQUIRE(mode == N2W_WALK_PREFIX || d_continuation_values, "RESIDUAL needs continuation values");
+    WalkArgs a = make_walk_args(*bvh, *problem, d_points, point_count, *options, mode == N2W_WALK_PREFIX ? 1 : 2);
+    for (int k = 0; k < 3; ++k) {
+      a.in_min[k] = input_min[k];
+      a.in_ext[k] = input_extent[k];
+    }
+    a.p_inputs = d_prefix_inputs;
+    a.p_boundary = d_boundary_values;
+    a.p_cont = d_continuation_values;
+    a.p_needs = d_needs_cache;
+    a.s_steps = d_step_count;
+    a.s_forced = d_forced_max_steps;
+    a.s_overflow = d_query_overflow;
+    run_walker(a, kOutPrefix, mode, *options, nullptr, nullptr, stream);
+  });
+}
+
+int n2w_wos_combine(const float* d_cache_outputs, const float* d_boundary_values,
+                    const float* d_continuation_values, const uint8_t* d_needs_cache,
+                    int64_t sample_count, float* d_nc_values, float* d_residual_values,
+                    int block_size, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(sample_count >= 0, "sample_count must be non-negative");
+    if (sample_count == 0) return;
+    N2W_REQUIRE(d_cache_outputs && d_boundary_values && d_continuation_values && d_needs_cache && d_nc_values &&
+                    d_residual_values,
+                "n2w_wos_combine: null pointer");
+    N2W_REQUIRE(block_size >= 1 && block_size <= 1024, "block_size must be in [1,1024]");
+    const int64_t grid = (sample_count + block_size - 1) / block_size;
+    combine_kernel<<<static_cast<unsigned>(grid), block_size, 0, stream>>>(
+        d_cache_outputs, d_boundary_values, d_continuation_values, d_needs_cache, sample_count, d_nc_values,
+        d_residual_values);
+    N2W_CUDA(cudaGetLastError());
+  });
+}
+
+int n2w_reduce_samples(const float* d_values, const int* d_step_count, const int* d_forced,
+                       int64_t point_count, int walks_per_point, n2w_point_stats stats, int accumulate,
+                       n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(point_count >= 0 && walks_per_point > 0, "invalid sizes");
+    if (point_count == 0) return;
+    N2W_REQUIRE(d_values && stats.d_sum && stats.d_sum_sq && stats.d_count, "n2w_reduce_samples: null pointer");
+    if (!accumulate) {
+      N2W_CUDA(cudaMemsetAsync(stats.d_sum, 0, sizeof(double) * point_count, stream));
+      N2W_CUDA(cudaMemsetAsync(stats.d_sum_sq, 0, sizeof(double) * point_count, stream));
+      N2W_CUDA(cudaMemsetAsync(stats.d_count, 0, sizeof(uint32_t) * point_count, stream));
+      if (stats.d_steps) N2W_CUDA(cudaMemsetAsync(stats.d_steps, 0, sizeof(uint64_t) * point_count, stream));
+      if (stats.d_forced) N2W_CUDA(cudaMemsetAsync(stats.d_forced, 0, sizeof(uint32_t) * point_count, stream));
+    }
+    const int64_t warps = point_count * ((walks_per_point + 1023) / 1024);
+    const int block = 256;
+    const int64_t grid = (warps * 32 + block - 1) / block;
+    reduce_samples_kernel<<<static_cast<unsigned>(grid), block, 0, stream>>>(
+        d_values, d_step_count, d_forced, point_count, walks_per_point, stats.d_sum, stats.d_sum_sq, stats.d_count,
+        d_step_count ? stats.d_steps : nullptr, d_forced ? stats.d_forced : nullptr);
+    N2W_CUDA(cudaGetLastError());
+  });
+}
+
+}  // extern "C"

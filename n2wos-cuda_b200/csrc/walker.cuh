@@ -1,0 +1,57 @@
+// Kernel argument block of the persistent walker (walker.cu).
+#pragma once
+
+#include <stdint.h>
+
+#include "n2w.h"
+
+namespace n2w {
+
+constexpr int kOutStats = 0;    // per-point FP64 accumulators
+constexpr int kOutSamples = 1;  // per-sample value / steps / flags (reference layout)
+constexpr int kOutPrefix = 2;   // per-sample prefix records for the cache levels
+
+constexpr int kWalkerMaxThreads = 256;
+constexpr int kDefaultWalkerThreads = 128;
+constexpr int kDefaultChunk = 8;
+
+struct WalkArgs {
+  const float4* nodes;
+  const float4* tris;
+  const n2w_vec3* points;
+  int64_t total_chunks;
+  int64_t chunks_per_point;
+  int walks_per_point;
+  int chunk;
+  int max_steps;
+  int depth_m;
+  float eps;
+  float step_scale;
+  uint32_t k0, k1;
+  int has_source;
+  int source_center;
+  int64_t deadline_ns;
+  n2w_problem problem;
+  // kOutStats
+  double* sum;
+  double* sum_sq;
+  uint32_t* count;
+  uint64_t* steps;
+  uint32_t* forced;
+  // kOutSamples / kOutPrefix
+  float* s_value;
+  int* s_steps;
+  int* s_forced;
+  int* s_overflow;
+  float* p_inputs;
+  float* p_boundary;
+  float* p_cont;
+  uint8_t* p_needs;
+  float in_min[3];
+  float in_ext[3];
+  // scratch
+  unsigned long long* queue;
+  n2w_walk_counters* counters;
+};
+
+}  // namespace n2w

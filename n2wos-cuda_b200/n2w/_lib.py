@@ -1,0 +1,164 @@
+"""ctypes binding of libn2w.so (the C ABI declared in include/n2w.h).
+
+The library is loaded from ``n2wos-cuda_b200/lib/libn2w.so``.  There is no
+fallback: if the shared library is missing the import raises, so a caller can
+never silently run a CPU path in its place.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parent.parent
+LIB_PATH = Path(os.environ.get("N2W_LIB", PKG_ROOT / "lib" / "libn2w.so"))
+
+if not LIB_PATH.exists():
+    raise ImportError(f"libn2w.so not found at {LIB_PATH}; build it with "
+                      f"'python n2wos-cuda_b200/build.py' (no CPU fallback exists)")
+
+lib = C.CDLL(str(LIB_PATH))
+
+N2W_OK, N2W_EINVAL, N2W_ECUDA, N2W_ENOMEM, N2W_ETIMEOUT, N2W_EIO, N2W_EINTERNAL = range(7)
+
+N2W_BC = {
+    "harmonic_x2_minus_y2": 0, "external_charges_medium": 1, "external_charges_high": 2,
+    "harmonic_zebra_k4": 3, "harmonic_zebra_k8": 4, "harmonic_zebra_k12": 5,
+    "external_charges_shell_k8": 6, "external_charges_shell_k16": 7,
+    "boundary_texture_stripes_k8": 8, "boundary_texture_stripes_k16": 9,
+    "boundary_texture_checker_k8": 10, "boundary_texture_checker_k16": 11,
+    "constant_one": 12, "poisson_multiscale": 30, "poisson_figlike_hf": 31,
+    "charges_seeded": 100, "poisson_sinprod": 101,
+}
+N2W_SOURCE_BALL, N2W_SOURCE_CENTER = 0, 1
+N2W_WALK_PURE, N2W_WALK_PREFIX, N2W_WALK_RESIDUAL = 0, 1, 2
+N2W_MAX_CHARGES = 16
+
+
+class N2wError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[n2w error {code}] {msg}")
+        self.code = code
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class BvhStats(C.Structure):
+    _fields_ = [("triangles", C.c_int64), ("nodes", C.c_int64), ("binary_nodes", C.c_int64),
+                ("leaves", C.c_int64), ("leaf_size", C.c_int32), ("max_depth", C.c_int32),
+                ("build_milliseconds", C.c_double), ("sah_cost", C.c_double),
+                ("device_bytes", C.c_int64)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("source_sampling", C.c_int32), ("charge_count", C.c_int32),
+                ("omega", C.c_float), ("charges", (C.c_float * 4) * N2W_MAX_CHARGES)]
+
+
+class WalkOptions(C.Structure):
+    _fields_ = [("walks_per_point", C.c_int32), ("max_steps", C.c_int32), ("depth_m", C.c_int32),
+                ("epsilon", C.c_float), ("step_scale", C.c_float), ("seed", C.c_uint64),
+                ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk", C.c_int32),
+                ("accumulate", C.c_int32), ("deadline_ns", C.c_int64)]
+
+
+class PointStats(C.Structure):
+    _fields_ = [("d_sum", C.c_void_p), ("d_sum_sq", C.c_void_p), ("d_count", C.c_void_p),
+                ("d_steps", C.c_void_p), ("d_forced", C.c_void_p)]
+
+
+class WalkCounters(C.Structure):
+    _fields_ = [(n, C.c_ulonglong) for n in
+                ("walks", "steps", "queries", "node_visits", "tri_tests", "overflow", "forced",
+                 "timed_out")]
+
+
+P = C.c_void_p
+I = C.c_int
+I64 = C.c_int64
+PP = C.POINTER(C.c_void_p)
+
+_SIGS = {
+    "n2w_last_error": (C.c_char_p, []),
+    "n2w_abi_version": (I, []),
+    "n2w_cuda_runtime_version_string": (I, [C.c_char_p, C.c_size_t]),
+    "n2w_cuda_device_summary": (I, [C.c_char_p, C.c_size_t]),
+    "n2w_mesh_create": (I, [P, I64, P, I64, C.c_char_p, PP]),
+    "n2w_mesh_bumpy_sphere_ref": (I, [I, I, C.c_float, PP]),
+    "n2w_mesh_bumpy_sphere_trig": (I, [I, I, C.c_float, I, I, PP]),
+    "n2w_mesh_icosphere_displaced": (I, [I, C.c_float, C.c_float, I, C.c_float, C.c_uint64, PP]),
+    "n2w_mesh_load_ply": (I, [C.c_char_p, PP]),
+    "n2w_mesh_load_obj": (I, [C.c_char_p, PP]),
+    "n2w_mesh_normalize": (I, [P, P, P]),
+    "n2w_mesh_counts": (I, [P, C.POINTER(I64), C.POINTER(I64)]),
+    "n2w_mesh_copy_out": (I, [P, P, P]),
+    "n2w_mesh_bounds": (I, [P, P]),
+    "n2w_mesh_count_degenerate": (I, [P, C.c_float, C.POINTER(I64)]),
+    "n2w_mesh_free": (None, [P]),
+    "n2w_bvh_host_build": (I, [P, I, C.c_char_p, PP]),
+    "n2w_bvh_host_stats": (I, [P, C.POINTER(BvhStats)]),
+    "n2w_bvh_host_copy": (I, [P, P, P]),
+    "n2w_bvh_host_free": (None, [P]),
+    "n2w_bvh_create": (I, [P, I, C.c_char_p, PP]),
+    "n2w_bvh_stats_get": (I, [P, C.POINTER(BvhStats)]),
+    "n2w_bvh_destroy": (None, [P]),
+    "n2w_bvh_query_device": (I, [P, P, I, P, P, P, P, I, P]),
+    "n2w_bvh_query_device_masked": (I, [P, P, P, I, P, P, P, P, I, P]),
+    "n2w_bvh_query_device_counted": (I, [P, P, I, P, P, P, P, P, P, I, P]),
+    "n2w_bvh_copy_layout": (I, [P, P, P]),
+    "n2w_bvh_inside_device": (I, [P, P, I, P, P, I, P]),
+    "n2w_slice_points": (I, [P, C.c_char_p, C.c_float, I, I, C.c_float, I, P, P]),
+    "n2w_problem_charges_seeded": (I, [I, C.c_float, C.c_float, C.c_uint64, C.POINTER(Problem)]),
+    "n2w_problem_sinprod": (I, [C.c_float, I, C.POINTER(Problem)]),
+    "n2w_problem_reference_mode": (I, [I, I, C.POINTER(Problem)]),
+    "n2w_problem_exact": (I, [C.POINTER(Problem), P, I64, P]),
+    "n2w_problem_eval_f32": (I, [C.POINTER(Problem), P, I64, P, P]),
+    "n2w_problem_mode_from_name": (I, [C.c_char_p, C.POINTER(I)]),
+    "n2w_problem_mode_name": (C.c_char_p, [I]),
+    "n2w_rng_philox4x32_10": (I, [P, C.c_uint64, C.c_uint32, P]),
+    "n2w_wos_workspace_bytes": (C.c_size_t, []),
+    "n2w_wos_estimate": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), PointStats, P, P, P]),
+    "n2w_wos_pure_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), P, P, P, P, P]),
+    "n2w_wos_prefix_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), I, P, P,
+                                   P, P, P, P, P, P, P, P]),
+    "n2w_wos_combine": (I, [P, P, P, P, I64, P, P, I, P]),
+    "n2w_reduce_samples": (I, [P, P, P, I64, I, PointStats, I, P]),
+    "n2w_device_count": (I, [C.POINTER(I)]),
+    "n2w_set_device": (I, [I]),
+    "n2w_malloc": (I, [PP, C.c_size_t]),
+    "n2w_free": (I, [P]),
+    "n2w_malloc_host": (I, [PP, C.c_size_t]),
+    "n2w_free_host": (I, [P]),
+    "n2w_memcpy_h2d": (I, [P, P, C.c_size_t, P]),
+    "n2w_memcpy_d2h": (I, [P, P, C.c_size_t, P]),
+    "n2w_memset": (I, [P, I, C.c_size_t, P]),
+    "n2w_stream_create": (I, [PP]),
+    "n2w_stream_destroy": (I, [P]),
+    "n2w_stream_sync": (I, [P]),
+    "n2w_device_sync": (I, []),
+    "n2w_timer_create": (I, [PP]),
+    "n2w_timer_start": (I, [P, P]),
+    "n2w_timer_stop": (I, [P, P]),
+    "n2w_timer_elapsed_ms": (I, [P, C.POINTER(C.c_float)]),
+    "n2w_timer_destroy": (None, [P]),
+    "n2w_sm_count": (I, [C.POINTER(I)]),
+    "n2w_mem_info": (I, [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+for _name, (_res, _args) in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def check(status: int) -> None:
+    if status != N2W_OK:
+        raise N2wError(status, lib.n2w_last_error().decode(errors="replace"))
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib, name)(*args))

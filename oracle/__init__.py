@@ -1,0 +1,236 @@
+"""ORACLE — test infrastructure only (the checker, never the product).
+
+numpy wrappers over liboracle.so (CPU restatement of the reference's hot path,
+oracle.cpp) and, when built, oracle/_ref/libn2wos_ref.so (the reference's own CPU
+sources) and oracle/_ref/libn2wos_ref_gpu.so (the reference's GPU kernel).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_lib = None
+_ref = None
+_ref_gpu = None
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            from . import build as _b
+            _b.build_oracle()
+        _lib = C.CDLL(str(path))
+    return _lib
+
+
+def ref_available() -> bool:
+    return (HERE / "_ref" / "libn2wos_ref.so").exists()
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(str(HERE / "_ref" / "libn2wos_ref.so"))
+        _ref.ref_bumpy_sphere.restype = C.c_void_p
+        _ref.ref_bumpy_sphere.argtypes = [C.c_int, C.c_int, C.c_float]
+        _ref.ref_load_ply.restype = C.c_void_p
+        _ref.ref_load_ply.argtypes = [C.c_char_p]
+        _ref.ref_load_obj.restype = C.c_void_p
+        _ref.ref_load_obj.argtypes = [C.c_char_p]
+        _ref.ref_mesh_from_arrays.restype = C.c_void_p
+        _ref.ref_mesh_from_arrays.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64]
+        _ref.ref_mesh_free.argtypes = [C.c_void_p]
+        _ref.ref_mesh_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        _ref.ref_mesh_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _ref.ref_normalize.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _ref.ref_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        _ref.ref_count_degenerate.restype = C.c_int64
+        _ref.ref_count_degenerate.argtypes = [C.c_void_p]
+        _ref.ref_host_bvh_stats.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        _ref.ref_last_error.restype = C.c_char_p
+    return _ref
+
+
+class RefMesh:
+    """A mesh owned by the reference library (n2wos::Mesh)."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise RuntimeError(ref().ref_last_error().decode())
+        self.h = C.c_void_p(handle)
+
+    @classmethod
+    def bumpy_sphere(cls, stacks, slices, amplitude=0.15):
+        return cls(ref().ref_bumpy_sphere(stacks, slices, amplitude))
+
+    @classmethod
+    def load_ply(cls, path):
+        return cls(ref().ref_load_ply(str(path).encode()))
+
+    @classmethod
+    def load_obj(cls, path):
+        return cls(ref().ref_load_obj(str(path).encode()))
+
+    @classmethod
+    def from_arrays(cls, v, t):
+        v = np.ascontiguousarray(v, np.float32)
+        t = np.ascontiguousarray(t, np.uint32)
+        return cls(ref().ref_mesh_from_arrays(_p(v), len(v), _p(t), len(t)))
+
+    def normalize(self):
+        c = np.zeros(3, np.float32)
+        s = np.zeros(1, np.float32)
+        if ref().ref_normalize(self.h, _p(c), _p(s)) != 0:
+            raise RuntimeError(ref().ref_last_error().decode())
+        return c, float(s[0])
+
+    def arrays(self):
+        nv, nt = C.c_int64(), C.c_int64()
+        ref().ref_mesh_counts(self.h, C.byref(nv), C.byref(nt))
+        v = np.empty((nv.value, 3), np.float32)
+        t = np.empty((nt.value, 3), np.uint32)
+        ref().ref_mesh_copy(self.h, _p(v), _p(t))
+        return v, t
+
+    def bruteforce(self, points):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        n = len(pts)
+        d2 = np.empty(n, np.float32)
+        cp = np.empty((n, 3), np.float32)
+        ids = np.empty(n, np.int32)
+        ref().ref_bruteforce(self.h, _p(pts), n, _p(d2), _p(cp), _p(ids))
+        return d2, cp, ids
+
+    def degenerate_count(self):
+        return int(ref().ref_count_degenerate(self.h))
+
+    def host_bvh_stats(self, leaf_size=8):
+        n, d = C.c_int64(), C.c_int32()
+        if ref().ref_host_bvh_stats(self.h, leaf_size, C.byref(n), C.byref(d)) != 0:
+            raise RuntimeError(ref().ref_last_error().decode())
+        return n.value, d.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.ref_mesh_free(self.h)
+            self.h = None
+
+
+def ref_gpu_available() -> bool:
+    return (HERE / "_ref" / "libn2wos_ref_gpu.so").exists()
+
+
+def ref_gpu():
+    global _ref_gpu
+    if _ref_gpu is None:
+        _ref_gpu = C.CDLL(str(HERE / "_ref" / "libn2wos_ref_gpu.so"))
+        _ref_gpu.ref_gpu_bvh_create.restype = C.c_void_p
+        _ref_gpu.ref_gpu_bvh_create.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int]
+        _ref_gpu.ref_gpu_query_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        _ref_gpu.ref_gpu_bvh_destroy.argtypes = [C.c_void_p]
+        _ref_gpu.ref_gpu_last_error.restype = C.c_char_p
+    return _ref_gpu
+
+
+# ---- the CPU restatement ---------------------------------------------------------
+
+def _setup():
+    L = lib()
+    L.oracle_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    L.oracle_traverse4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    L.oracle_philox4x32_10.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+    L.oracle_closest_point_on_triangle.argtypes = [C.c_void_p] * 5
+    L.oracle_wos.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                             C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_int]
+    return L
+
+
+def bruteforce(vertices, triangles, points, threads=8):
+    """Brute-force closest point with tie counts (reference closest_point.cpp:50-68)."""
+    L = _setup()
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    n = len(pts)
+    d2 = np.empty(n, np.float32)
+    cp = np.empty((n, 3), np.float32)
+    ids = np.empty(n, np.int32)
+    ties = np.empty(n, np.int32)
+    L.oracle_bruteforce(_p(v), _p(t), len(t), _p(pts), n, _p(d2), _p(cp), _p(ids), _p(ties), threads)
+    return {"distance2": d2, "closest": cp, "triangle_id": ids, "ties": ties}
+
+
+def traverse4(nodes, tris, points, threads=8):
+    """The product's 4-wide traversal restated on the CPU (visit counts)."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    n = len(pts)
+    d2 = np.empty(n, np.float32)
+    cp = np.empty((n, 3), np.float32)
+    ids = np.empty(n, np.int32)
+    nv = np.empty(n, np.int32)
+    nt = np.empty(n, np.int32)
+    L.oracle_traverse4(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(tris)), _p(pts), n, _p(d2),
+                       _p(cp), _p(ids), _p(nv), _p(nt), threads)
+    return {"distance2": d2, "closest": cp, "triangle_id": ids, "node_visits": nv, "tri_tests": nt}
+
+
+def inside_bruteforce(vertices, triangles, points, threads=8):
+    """Reference +x ray-parity mask over all triangles (cubql_bvh.cu:407-455)."""
+    L = lib()
+    L.oracle_inside_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                           C.c_void_p, C.c_int]
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    out = np.empty(len(pts), np.uint8)
+    L.oracle_inside_bruteforce(_p(v), _p(t), len(t), _p(pts), len(pts), _p(out), threads)
+    return out
+
+
+def philox(ctr, k0, k1):
+    L = _setup()
+    c = np.ascontiguousarray(ctr, np.uint32)
+    out = np.empty(4, np.uint32)
+    L.oracle_philox4x32_10(_p(c), k0, k1, _p(out))
+    return out
+
+
+def closest_point_on_triangle(p, a, b, c):
+    L = _setup()
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (p, a, b, c)]
+    out = np.empty(3, np.float32)
+    L.oracle_closest_point_on_triangle(*[_p(x) for x in arrs], _p(out))
+    return out
+
+
+def wos(nodes, tris, problem_bytes, points, walks_per_point, max_steps, eps, step_scale, k0, k1, threads=8):
+    """Scalar CPU WoS (reference nc_wos_from_point semantics); per-point FP64 sums."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    n = len(pts)
+    s = np.empty(n, np.float64)
+    s2 = np.empty(n, np.float64)
+    st = np.empty(n, np.float64)
+    pb = np.frombuffer(problem_bytes, dtype=np.uint8).copy()
+    L.oracle_wos(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(tris)), _p(pb), _p(pts), n,
+                 walks_per_point, max_steps, eps, step_scale, k0, k1, _p(s), _p(s2), _p(st), threads)
+    W = float(walks_per_point)
+    mean = s / W
+    var = np.maximum((s2 - W * mean * mean) / max(W - 1, 1), 0.0)
+    return {"mean": mean, "sample_variance": var, "stderr": np.sqrt(var / W), "mean_steps": st / W,
+            "sum": s, "sum_sq": s2, "steps": st}

@@ -1,0 +1,132 @@
+"""GPU closest-point parity (through the C ABI) against the oracle and the
+reference's own brute-force outputs: distance2, closest point and triangle id
+bit-exact (lowest id on exact ties, like the reference brute force)."""
+import ctypes as C
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import uniform_box
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_bitexact(got, want):
+    assert np.array_equal(got["distance2"].view(np.uint32), want["distance2"].view(np.uint32))
+    assert np.array_equal(got["closest"].view(np.uint32), want["closest"].view(np.uint32))
+    assert np.array_equal(got["triangle_id"], want["triangle_id"])
+
+
+@pytest.fixture(scope="module")
+def ref_bvh(gpu, bumpy_ref_mesh):
+    return gpu.Bvh(bumpy_ref_mesh, 4, "sah")
+
+
+def test_golden_reference_vectors(gpu, ref_bvh, golden_closest):
+    r = ref_bvh.query(golden_closest["points"])
+    assert_bitexact(r, golden_closest)
+    assert not r["overflow"].any()
+
+
+@pytest.mark.parametrize("method,leaf", [("sah", 4), ("sah", 1), ("sah", 8), ("spatial_median", 8)])
+def test_config0_queries_vs_oracle(gpu, method, leaf):
+    """BASELINE config-0 geometry: trig bumpy sphere 128x256, 262,144 uniform
+    queries in [-1.2,1.2]^3; all compared with the CPU restatement over the same
+    layout, and 2,048 with the brute force."""
+    m = gpu.Mesh.bumpy_sphere_trig(128, 256, 0.08, 6, 8)
+    m.normalize()
+    v, t = m.arrays()
+    bvh = gpu.Bvh(m, leaf, method)
+    pts = uniform_box(262144, 1.2, 12345)
+    r = bvh.query(pts, counted=True)
+    nodes, tris = bvh.layout()
+    tr = oracle.traverse4(nodes, tris, pts)
+    assert_bitexact(r, tr)
+    assert np.array_equal(r["node_visits"], tr["node_visits"])
+    assert np.array_equal(r["tri_tests"], tr["tri_tests"])
+    bf = oracle.bruteforce(v, t, pts[:2048])
+    sub = {k: r[k][:2048] for k in ("distance2", "closest", "triangle_id")}
+    assert_bitexact(sub, bf)
+    print(f"ties among 2048 validation points: {(bf['ties'] > 1).sum()}")
+
+
+def test_query_modes_surface_and_shell(gpu):
+    m = gpu.Mesh.icosphere_displaced(5, 0.12, 3.0, 4, 0.5, 7)
+    m.normalize()
+    v, t = m.arrays()
+    bvh = gpu.Bvh(m, 4, "sah")
+    rng = np.random.default_rng(9)
+    tri = t[rng.integers(0, len(t), 3000)]
+    w = rng.dirichlet([1, 1, 1], 3000)
+    surf = (v[tri[:, 0]] * w[:, :1] + v[tri[:, 1]] * w[:, 1:2] + v[tri[:, 2]] * w[:, 2:]).astype(np.float32)
+    shell = surf * (1 + rng.uniform(-1e-3, 1e-3, (3000, 1))).astype(np.float32)
+    pts = np.concatenate([surf, shell, v[:1000]])
+    assert_bitexact(bvh.query(pts), oracle.bruteforce(v, t, pts))
+
+
+def test_masked_query(gpu, ref_bvh, golden_closest):
+    pts = golden_closest["points"]
+    active = (np.arange(len(pts)) % 3 != 0).astype(np.uint8)
+    r = ref_bvh.query(pts, active=active)
+    off = active == 0
+    assert np.all(r["distance2"][off] == 0) and np.all(r["triangle_id"][off] == -1)
+    assert np.array_equal(r["closest"][off], pts[off]) and np.all(r["overflow"][off] == 0)
+    on = ~off
+    assert np.array_equal(r["distance2"][on], golden_closest["distance2"][on])
+    assert np.array_equal(r["triangle_id"][on], golden_closest["triangle_id"][on])
+
+
+def test_argument_errors(gpu, ref_bvh):
+    from n2w._lib import lib
+
+    d = gpu.DeviceBuffer(4096)
+    h = ref_bvh.handle
+    assert lib.n2w_bvh_query_device(h, d.ptr, 0, d.ptr, d.ptr, d.ptr, d.ptr, 128, None) == 0
+    assert lib.n2w_bvh_query_device(h, d.ptr, -1, d.ptr, d.ptr, d.ptr, d.ptr, 128, None) == 1
+    assert lib.n2w_bvh_query_device(h, None, 4, d.ptr, d.ptr, d.ptr, d.ptr, 128, None) == 1
+    assert lib.n2w_bvh_query_device(h, d.ptr, 4, d.ptr, d.ptr, d.ptr, d.ptr, 0, None) == 1
+    assert lib.n2w_bvh_query_device(h, d.ptr, 4, d.ptr, d.ptr, d.ptr, d.ptr, 1025, None) == 1
+    assert lib.n2w_bvh_query_device(None, d.ptr, 4, d.ptr, d.ptr, d.ptr, d.ptr, 128, None) == 1
+
+
+@pytest.mark.parametrize("block", [1, 32, 96, 1024])
+def test_block_sizes(gpu, ref_bvh, golden_closest, block):
+    assert_bitexact(ref_bvh.query(golden_closest["points"], block_size=block), golden_closest)
+
+
+def test_inside_classification_matches_reference_rule(gpu):
+    m = gpu.Mesh.bumpy_sphere_trig(48, 96, 0.08, 6, 8)
+    m.normalize()
+    v, t = m.arrays()
+    bvh = gpu.Bvh(m, 4, "sah")
+    pts = uniform_box(20000, 1.1, 4)
+    lo, hi = m.bounds()
+    grid, _ = gpu.slice_points(lo, hi, "xy", 0.12, 64, 64)
+    pts = np.concatenate([pts, grid])
+    got = bvh.inside(pts)
+    want = oracle.inside_bruteforce(v, t, pts)
+    assert np.array_equal(got, want)
+    r = np.linalg.norm(pts, axis=1)
+    assert got[r < 0.8].all() and not got[r > 1.0001].any()
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="reference GPU kernel not built")
+def test_reference_gpu_kernel_agrees(gpu, bumpy_ref_mesh, golden_closest):
+    """The reference's own GPU kernel (bvh_query.cu, compiled for sm_100a) on the
+    same device: distances within its own 2e-4 acceptance of ours."""
+    v, t = bumpy_ref_mesh.arrays()
+    R = oracle.ref_gpu()
+    h = R.ref_gpu_bvh_create(v.ctypes.data, len(v), t.ctypes.data, len(t), 8)
+    assert h, R.ref_gpu_last_error()
+    try:
+        pts = golden_closest["points"]
+        n = len(pts)
+        dp = gpu.DeviceBuffer.from_array(pts)
+        dd, dc, di, do = gpu.DeviceBuffer(4 * n), gpu.DeviceBuffer(12 * n), gpu.DeviceBuffer(4 * n), gpu.DeviceBuffer(4 * n)
+        assert R.ref_gpu_query_device(h, dp.ptr, n, dd.ptr, dc.ptr, di.ptr, do.ptr, 128, None) == 0
+        d2 = dd.download(np.float32)
+        assert np.max(np.abs(np.sqrt(d2) - np.sqrt(golden_closest["distance2"]))) <= 2e-4
+    finally:
+        R.ref_gpu_bvh_destroy(C.c_void_p(h))
