@@ -192,6 +192,9 @@ def main():
     ap.add_argument("--impl", default="n2w", choices=["n2w", "reference"])
     ap.add_argument("--walks", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=0,
+                    help="use only the first N slice points (smaller workload for profiler captures; "
+                         "the default 0 runs the full slice)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -214,13 +217,16 @@ def main():
 
     call("n2w_set_device", local)
     mesh, bvh, pts, problem, exact, frame = build_scene(n2w, lib, call)
+    if args.points > 0:
+        sel = np.linspace(0, len(pts) - 1, min(args.points, len(pts))).astype(np.int64)
+        pts, exact = np.ascontiguousarray(pts[sel]), exact[sel]
     n = len(pts)
     W = args.walks
     stream = n2w.Stream()
     d_pts = n2w.DeviceBuffer.from_array(pts)
     stats = n2w.PointStatsBuffers.allocate(n)
     d_cnt = n2w.DeviceBuffer(C.sizeof(n2w._lib.WalkCounters))
-    d_ws = n2w.DeviceBuffer(lib.n2w_wos_workspace_bytes())
+    d_ws = n2w.DeviceBuffer(lib.n2w_wos_workspace_bytes(n))
     flush = n2w.DeviceBuffer(256 << 20)
     opts = n2w.walk_options(walks_per_point=W, max_steps=256, epsilon=5e-4, step_scale=0.999,
                             seed=12345 + 1000003 * rank)

@@ -145,6 +145,10 @@ int n2w_bvh_inside_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int quer
  * frame_out[4] = u_min, u_max, v_min, v_max (may be NULL). */
 int n2w_slice_points(const float* bounds6, const char* view, float plane, int width, int height,
                      float padding_fraction, int preserve_aspect, float* points_out, float* frame_out);
+/* Seed grid built with the BVH: (n+1)^3 lattice nodes lo + h*(i,j,k); slot of
+ * the triangle nearest each node (leaf order).  Queries test that triangle first,
+ * so their traversal starts with a tight bound.  Any output may be NULL. */
+int n2w_bvh_seed_grid(const n2w_bvh* bvh, float* lo_out, float* h_out, int* n_out, int* slots_out);
 /* Copies the device layout back to the host: nodes (128 B each) and leaf-ordered
  * triangles (48 B each).  Either pointer may be NULL.  Used by the CPU restatement
  * of the traversal to count visits. */
@@ -217,6 +221,8 @@ typedef struct n2w_walk_options {
   int32_t chunk;         /* walks a lane takes per queue pop (0 = tuned default) */
   int32_t accumulate;    /* 0: outputs are overwritten; 1: results are added */
   int64_t deadline_ns;   /* 0 = none; else walkers stop this many ns after launch */
+  int32_t regen_threshold; /* lanes of a warp that must be waiting before walk
+                              updates / regeneration run (1..32; 0 = tuned default) */
 } n2w_walk_options;
 
 /* Per-point FP64 estimator accumulators (device arrays, one entry per point). */
@@ -246,8 +252,9 @@ typedef struct n2w_walk_counters {
  * random numbers of walk w = point*W + j at step s: ctr = {w, w>>32, s, 0|1}. */
 int n2w_rng_philox4x32_10(const uint32_t* ctr, uint64_t seed, uint32_t tag, uint32_t* out);
 
-/* Workspace bytes the walker needs (work-queue counter + counters). */
-size_t n2w_wos_workspace_bytes(void);
+/* Workspace bytes a walker call over point_count points needs: the work-queue
+ * counter, run counters and each point's first closest-point query (24 B). */
+size_t n2w_wos_workspace_bytes(int64_t point_count);
 
 /* Plain WoS estimate of u at each point with per-point FP64 reductions on the
  * device: persistent walker, counter-based Philox RNG, queue regeneration.

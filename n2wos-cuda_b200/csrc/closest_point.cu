@@ -1,9 +1,12 @@
 // Device-pointer closest-point queries over the 4-wide BVH (reference
 // CudaBvh::query_device, src/cuda/bvh_query.cu:228-261, and the masked cuBQL
-// variant, src/cuda/cubql_bvh.cu:187-214).  One thread per query, ordered
-// traversal with the stack in per-thread local memory (geom.cuh).
+// variant, src/cuda/cubql_bvh.cu:187-214).  One thread per query: the query is
+// seeded with the triangle stored at the nearest seed-grid node (a real
+// candidate, so the exact answer is unchanged), then an ordered traversal with
+// the stack in per-thread local memory (geom.cuh) finishes it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 
@@ -11,11 +14,23 @@
 #include "internal.hpp"
 
 namespace n2w {
+
+dev::SeedGrid seed_grid_of(const n2w_bvh& b) {
+  dev::SeedGrid g;
+  g.slots = b.d_seed;
+  g.lo_x = b.seed_lo[0];
+  g.lo_y = b.seed_lo[1];
+  g.lo_z = b.seed_lo[2];
+  g.inv_h = b.seed_h > 0.0f ? 1.0f / b.seed_h : 0.0f;
+  g.n = b.seed_n;
+  return g;
+}
+
 namespace {
 
 template <bool kMasked, bool kCount>
-__global__ void __launch_bounds__(256) closest_point_kernel(
-    const float4* __restrict__ nodes, const float4* __restrict__ tris,
+__global__ void __launch_bounds__(1024) closest_point_kernel(
+    const float4* __restrict__ nodes, const float4* __restrict__ tris, const dev::SeedGrid grid,
     const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
     float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
     int* __restrict__ out_overflow, int* __restrict__ out_nodes, int* __restrict__ out_tris) {
@@ -33,12 +48,18 @@ __global__ void __launch_bounds__(256) closest_point_kernel(
     }
     return;
   }
+  const dev::V3 p = dev::v3(pt.x, pt.y, pt.z);
   dev::ClosestHit hit;
   hit.d2 = FLT_MAX;
   hit.id = INT32_MAX;
+  hit.slot = -1;
   hit.cp = dev::v3(0.0f, 0.0f, 0.0f);
   dev::TraversalStats st{0, 0, 0};
-  dev::traverse<kCount>(nodes, tris, dev::v3(pt.x, pt.y, pt.z), hit, st);
+  if (grid.slots) {
+    dev::test_slot(tris, dev::seed_slot(grid, p), p, hit);
+    if (kCount) ++st.tri_tests;
+  }
+  dev::traverse<kCount>(nodes, tris, p, hit, st);
   out_d2[q] = hit.d2;
   out_cp[q] = n2w_vec3{hit.cp.x, hit.cp.y, hit.cp.z};
   out_id[q] = hit.id == INT32_MAX ? -1 : hit.id;
@@ -49,12 +70,38 @@ __global__ void __launch_bounds__(256) closest_point_kernel(
   }
 }
 
+// Builds the seed grid: a cold exact query at every lattice node.
+__global__ void __launch_bounds__(256) seed_grid_kernel(const float4* __restrict__ nodes,
+                                                        const float4* __restrict__ tris, float lox, float loy,
+                                                        float loz, float h, int n, int* __restrict__ slots,
+                                                        int* __restrict__ overflow) {
+  const int s = n + 1;
+  const int64_t total = static_cast<int64_t>(s) * s * s;
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int ix = static_cast<int>(i % s), iy = static_cast<int>((i / s) % s), iz = static_cast<int>(i / (static_cast<int64_t>(s) * s));
+  // Lattice position lo + h * i, rounded per operation (no FMA) so a host
+  // float32 evaluation of the same expression gives the same point.
+  const dev::V3 p = dev::v3(__fadd_rn(lox, __fmul_rn(h, static_cast<float>(ix))),
+                            __fadd_rn(loy, __fmul_rn(h, static_cast<float>(iy))),
+                            __fadd_rn(loz, __fmul_rn(h, static_cast<float>(iz))));
+  dev::ClosestHit hit;
+  hit.d2 = FLT_MAX;
+  hit.id = INT32_MAX;
+  hit.slot = 0;
+  hit.cp = p;
+  dev::TraversalStats st{0, 0, 0};
+  dev::traverse<false>(nodes, tris, p, hit, st);
+  slots[i] = hit.slot;
+  if (st.overflow) atomicOr(overflow, 1);
+}
+
 // Inside/outside by ray parity along +x with the reference's deterministic
 // offset (src/cuda/cubql_bvh.cu:446-455).
-__global__ void __launch_bounds__(256) inside_kernel(const float4* __restrict__ nodes,
-                                                     const float4* __restrict__ tris,
-                                                     const n2w_vec3* __restrict__ points, int n,
-                                                     uint8_t* __restrict__ inside, int* __restrict__ overflow) {
+__global__ void __launch_bounds__(1024) inside_kernel(const float4* __restrict__ nodes,
+                                                      const float4* __restrict__ tris,
+                                                      const n2w_vec3* __restrict__ points, int n,
+                                                      uint8_t* __restrict__ inside, int* __restrict__ overflow) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const n2w_vec3 p = points[q];
@@ -81,15 +128,16 @@ void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const ui
   const int grid = (n + block_size - 1) / block_size;
   const float4* nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
   const float4* tris = reinterpret_cast<const float4*>(bvh.d_tris);
+  const dev::SeedGrid sg = seed_grid_of(bvh);
   if (d_nodes) {
     closest_point_kernel<false, true><<<grid, block_size, 0, stream>>>(
-        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, d_nodes, d_tris);
+        nodes, tris, sg, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, d_nodes, d_tris);
   } else if (d_active) {
     closest_point_kernel<true, false><<<grid, block_size, 0, stream>>>(
-        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
+        nodes, tris, sg, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
   } else {
     closest_point_kernel<false, false><<<grid, block_size, 0, stream>>>(
-        nodes, tris, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
+        nodes, tris, sg, d_points, d_active, n, d_d2, d_cp, d_id, d_overflow, nullptr, nullptr);
   }
   N2W_CUDA(cudaGetLastError());
 }
@@ -99,6 +147,37 @@ int sm_count_current() {
   N2W_CUDA(cudaGetDevice(&dev));
   N2W_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   return sms;
+}
+
+// Seed grid over the mesh box grown by 20 % of its largest extent on every side.
+void build_seed_grid(n2w_bvh& b, const n2w_mesh& mesh, int n) {
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const auto& v : mesh.vertices) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], v[a]);
+      hi[a] = std::max(hi[a], v[a]);
+    }
+  }
+  const float ext = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+  const float pad = 0.2f * ext + 1e-6f;
+  const float h = (ext + 2.0f * pad) / static_cast<float>(n);
+  for (int a = 0; a < 3; ++a) b.seed_lo[a] = 0.5f * (lo[a] + hi[a]) - 0.5f * (ext + 2.0f * pad);
+  b.seed_h = h;
+  b.seed_n = n;
+  const int64_t total = static_cast<int64_t>(n + 1) * (n + 1) * (n + 1);
+  N2W_CUDA(cudaMalloc(&b.d_seed, total * sizeof(int)));
+  int* d_ov = nullptr;
+  N2W_CUDA(cudaMalloc(&d_ov, sizeof(int)));
+  N2W_CUDA(cudaMemset(d_ov, 0, sizeof(int)));
+  const int block = 256;
+  seed_grid_kernel<<<static_cast<unsigned>((total + block - 1) / block), block>>>(
+      reinterpret_cast<const float4*>(b.d_nodes), reinterpret_cast<const float4*>(b.d_tris), b.seed_lo[0],
+      b.seed_lo[1], b.seed_lo[2], h, n, b.d_seed, d_ov);
+  N2W_CUDA(cudaGetLastError());
+  int ov = 0;
+  N2W_CUDA(cudaMemcpy(&ov, d_ov, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d_ov);
+  if (ov) throw Error(N2W_EINTERNAL, "traversal stack overflow while building the seed grid");
 }
 
 }  // namespace n2w
@@ -114,6 +193,13 @@ void check_query_args(const n2w_bvh* bvh, const void* pts, int n, const void* d2
   if (n == 0) return;
   N2W_REQUIRE(pts && d2 && cp && id && ov, "query_device received a null device pointer");
   N2W_REQUIRE(block_size >= 1 && block_size <= 1024, "CUDA block size must be in [1, 1024]");
+}
+
+void release(n2w_bvh* b) {
+  if (b->d_nodes) cudaFree(b->d_nodes);
+  if (b->d_tris) cudaFree(b->d_tris);
+  if (b->d_seed) cudaFree(b->d_seed);
+  delete b;
 }
 
 }  // namespace
@@ -132,14 +218,15 @@ int n2w_bvh_create(const n2w_mesh* mesh, int leaf_size, const char* build_method
       N2W_CUDA(cudaMalloc(&b->d_tris, h.tris.size() * sizeof(TriRec)));
       N2W_CUDA(cudaMemcpy(b->d_nodes, h.nodes.data(), h.nodes.size() * sizeof(Node4), cudaMemcpyHostToDevice));
       N2W_CUDA(cudaMemcpy(b->d_tris, h.tris.data(), h.tris.size() * sizeof(TriRec), cudaMemcpyHostToDevice));
+      build_seed_grid(*b, *mesh, kSeedGridCells);
+      N2W_CUDA(cudaDeviceSynchronize());
     } catch (...) {
-      if (b->d_nodes) cudaFree(b->d_nodes);
-      if (b->d_tris) cudaFree(b->d_tris);
-      delete b;
+      release(b);
       throw;
     }
     const auto t1 = std::chrono::steady_clock::now();
     b->stats = host_stats(h, leaf_size, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    b->stats.device_bytes += static_cast<int64_t>(kSeedGridCells + 1) * (kSeedGridCells + 1) * (kSeedGridCells + 1) * 4;
     *out = b;
   });
 }
@@ -152,10 +239,7 @@ int n2w_bvh_stats_get(const n2w_bvh* bvh, n2w_bvh_stats* out) {
 }
 
 void n2w_bvh_destroy(n2w_bvh* bvh) {
-  if (!bvh) return;
-  if (bvh->d_nodes) cudaFree(bvh->d_nodes);
-  if (bvh->d_tris) cudaFree(bvh->d_tris);
-  delete bvh;
+  if (bvh) release(bvh);
 }
 
 int n2w_bvh_query_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int query_count,
@@ -217,6 +301,19 @@ int n2w_bvh_copy_layout(const n2w_bvh* bvh, void* nodes_out, void* tris_out) {
     if (tris_out) {
       N2W_CUDA(cudaMemcpy(tris_out, bvh->d_tris, static_cast<size_t>(bvh->stats.triangles) * sizeof(TriRec),
                           cudaMemcpyDeviceToHost));
+    }
+  });
+}
+
+int n2w_bvh_seed_grid(const n2w_bvh* bvh, float* lo_out, float* h_out, int* n_out, int* slots_out) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && bvh->d_seed, "BVH has no seed grid");
+    if (lo_out) std::memcpy(lo_out, bvh->seed_lo, sizeof(bvh->seed_lo));
+    if (h_out) *h_out = bvh->seed_h;
+    if (n_out) *n_out = bvh->seed_n;
+    if (slots_out) {
+      const size_t s = static_cast<size_t>(bvh->seed_n) + 1;
+      N2W_CUDA(cudaMemcpy(slots_out, bvh->d_seed, s * s * s * sizeof(int), cudaMemcpyDeviceToHost));
     }
   });
 }

@@ -38,48 +38,56 @@ __device__ __forceinline__ V3 vscale(V3 a, float s) { return V3{fm(a.x, s), fm(a
 __device__ __forceinline__ float vdot(V3 a, V3 b) { return fa(fa(fm(a.x, b.x), fm(a.y, b.y)), fm(a.z, b.z)); }
 
 // Ericson closest point on triangle abc to p, reference operation order.
+// Branch-free form for SIMT: all six dot products and the three barycentric
+// numerators are computed, the Voronoi region is chosen with Ericson's tests in
+// his order, and only the chosen region's expression is evaluated (one IEEE
+// division); each region's result uses exactly the reference's operations:
+//   edge ab: a + ab*(d1/(d1-d3))           edge ac: a + ac*(d2/(d2-d6))
+//   edge bc: b + (c-b)*((d4-d3)/((d4-d3)+(d5-d6)))
+//   face:    (a + ab*(vb*r)) + ac*(vc*r),  r = 1/((va+vb)+vc)
+//   vertex regions return the vertex itself.
 __device__ __forceinline__ V3 closest_point_triangle(V3 p, V3 a, V3 b, V3 c) {
   const V3 ab = vsub(b, a);
   const V3 ac = vsub(c, a);
   const V3 ap = vsub(p, a);
   const float d1 = vdot(ab, ap);
   const float d2 = vdot(ac, ap);
-  if (d1 <= 0.0f && d2 <= 0.0f) return a;
-
   const V3 bp = vsub(p, b);
   const float d3 = vdot(ab, bp);
   const float d4 = vdot(ac, bp);
-  if (d3 >= 0.0f && d4 <= d3) return b;
-
+  const V3 cq = vsub(p, c);
+  const float d5 = vdot(ab, cq);
+  const float d6 = vdot(ac, cq);
   const float vc = fs(fm(d1, d4), fm(d3, d2));
-  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-    const float v = fd(d1, fs(d1, d3));
-    return vadd(a, vscale(ab, v));
-  }
-
-  const V3 cp = vsub(p, c);
-  const float d5 = vdot(ab, cp);
-  const float d6 = vdot(ac, cp);
-  if (d6 >= 0.0f && d5 <= d6) return c;
-
   const float vb = fs(fm(d5, d2), fm(d1, d6));
-  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-    const float w = fd(d2, fs(d2, d6));
-    return vadd(a, vscale(ac, w));
-  }
-
   const float va = fs(fm(d3, d6), fm(d5, d4));
   const float d43 = fs(d4, d3);
   const float d56 = fs(d5, d6);
-  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) {
-    const float w = fd(d43, fa(d43, d56));
-    return vadd(b, vscale(vsub(c, b), w));
-  }
 
-  const float denom = fd(1.0f, fa(fa(va, vb), vc));
-  const float v = fm(vb, denom);
-  const float w = fm(vc, denom);
-  return vadd(vadd(a, vscale(ab, v)), vscale(ac, w));
+  const bool rA = d1 <= 0.0f && d2 <= 0.0f;
+  const bool rB = !rA && d3 >= 0.0f && d4 <= d3;
+  const bool rAB = !rA && !rB && vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f;
+  const bool r3 = rA || rB || rAB;
+  const bool rC = !r3 && d6 >= 0.0f && d5 <= d6;
+  const bool rAC = !r3 && !rC && vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f;
+  const bool rBC = !r3 && !rC && !rAC && va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f;
+  const bool rF = !r3 && !rC && !rAC && !rBC;
+
+  float num = 0.0f, den = 1.0f;
+  if (rAB) { num = d1; den = fs(d1, d3); }
+  if (rAC) { num = d2; den = fs(d2, d6); }
+  if (rBC) { num = d43; den = fa(d43, d56); }
+  if (rF) { num = 1.0f; den = fa(fa(va, vb), vc); }
+  const float q = fd(num, den);
+  const float s = rF ? fm(vb, q) : q;
+  const V3 base = rBC ? b : a;
+  const V3 e1 = rBC ? vsub(c, b) : (rAC ? ac : ab);
+  V3 r = vadd(base, vscale(e1, s));
+  if (rF) r = vadd(r, vscale(ac, fm(vc, q)));
+  if (rA) r = a;
+  if (rB) r = b;
+  if (rC) r = c;
+  return r;
 }
 
 // Squared distance from p to box [lo, hi] along one axis pair; +inf for empty slots.
@@ -108,9 +116,49 @@ __device__ __forceinline__ void cswap(float& da, int& ra, float& db, int& rb) {
 
 struct ClosestHit {
   float d2;
-  int id;  // original triangle id; INT32_MAX when nothing was found below the bound
+  int id;    // original triangle id; INT32_MAX when nothing was found below the bound
+  int slot;  // leaf-order index of that triangle (used to re-seed the next query)
   V3 cp;
 };
+
+// Tests one triangle (by leaf-order slot) and keeps it if it beats the hit in
+// (d2, id) order.  Seeding a query with real candidates gives the traversal a
+// tight bound without changing its answer.
+__device__ __forceinline__ void test_slot(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
+  const float4* t = tris + static_cast<size_t>(slot) * 3;
+  const float4 a = __ldg(t + 0);
+  const float4 b = __ldg(t + 1);
+  const float4 c = __ldg(t + 2);
+  const V3 cp = closest_point_triangle(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z));
+  const V3 dv = vsub(cp, p);
+  const float dd = vdot(dv, dv);
+  const int id = __float_as_int(a.w);
+  if (dd < hit.d2 || (dd == hit.d2 && id < hit.id)) {
+    hit.d2 = dd;
+    hit.id = id;
+    hit.slot = slot;
+    hit.cp = cp;
+  }
+}
+
+// Seed grid: (n+1)^3 lattice nodes over a padded mesh box; node value = leaf
+// slot of the triangle closest to the node.  The nearest node's triangle is a
+// candidate within (node distance + |x - node|) of x.
+struct SeedGrid {
+  const int* slots;  // nullptr when absent
+  float lo_x, lo_y, lo_z;
+  float inv_h;
+  int n;  // cells per axis
+};
+
+__device__ __forceinline__ int seed_slot(const SeedGrid& g, V3 p) {
+  const float fx = (p.x - g.lo_x) * g.inv_h, fy = (p.y - g.lo_y) * g.inv_h, fz = (p.z - g.lo_z) * g.inv_h;
+  const int ix = __float2int_rn(fminf(fmaxf(fx, 0.0f), static_cast<float>(g.n)));
+  const int iy = __float2int_rn(fminf(fmaxf(fy, 0.0f), static_cast<float>(g.n)));
+  const int iz = __float2int_rn(fminf(fmaxf(fz, 0.0f), static_cast<float>(g.n)));
+  const int s = g.n + 1;
+  return __ldg(g.slots + (static_cast<size_t>(iz) * s + iy) * s + ix);
+}
 
 struct TraversalStats {
   int node_visits;
@@ -182,6 +230,7 @@ __device__ __forceinline__ void traverse(const float4* __restrict__ nodes,
         if (dd < hit.d2 || (dd == hit.d2 && id < hit.id)) {
           hit.d2 = dd;
           hit.id = id;
+          hit.slot = first + i;
           hit.cp = cp;
         }
       }

@@ -21,6 +21,10 @@ struct n2w_mesh {
 struct n2w_bvh {
   n2w::Node4* d_nodes = nullptr;
   n2w::TriRec* d_tris = nullptr;
+  int* d_seed = nullptr;  // seed grid: leaf slot of the nearest triangle per lattice node
+  float seed_lo[3] = {0, 0, 0};
+  float seed_h = 0.0f;
+  int seed_n = 0;
   n2w_bvh_stats stats{};
   int device = 0;
 };
@@ -87,6 +91,8 @@ n2w_bvh_stats host_stats(const HostBvh& h, int leaf_size, double ms);
 void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const uint8_t* d_active,
                           int n, float* d_d2, n2w_vec3* d_cp, int* d_id, int* d_overflow,
                           int* d_nodes, int* d_tris, int block_size, cudaStream_t stream);
+
+void build_seed_grid(n2w_bvh& b, const n2w_mesh& mesh, int n);
 
 void launch_inside(const n2w_bvh& bvh, const n2w_vec3* d_points, int n, uint8_t* d_inside, int* d_overflow,
                    int block_size, cudaStream_t stream);

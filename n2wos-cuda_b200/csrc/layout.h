@@ -27,6 +27,7 @@ namespace n2w {
 constexpr int32_t kEmptyChild = INT32_MIN;
 constexpr int kMaxLeafSize = 8;
 constexpr int kTraversalStack = 64;
+constexpr int kSeedGridCells = 128;  // seed-grid cells per axis
 
 struct alignas(128) Node4 {
   float lo_x[4];

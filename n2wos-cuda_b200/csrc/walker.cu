@@ -13,9 +13,10 @@
 //    never idle a lane while work remains;
 //  * counter-based Philox keyed by (seed; walk id, step, stream), so a walk's
 //    path is independent of scheduling (serving "alone == in the mix");
-//  * every query after the first is warm-started with the squared distance to
-//    the previous closest point (an upper bound of the new distance), which
-//    prunes the BVH to the walker's neighbourhood without changing the result;
+//  * the first query of every walk of a point is computed once per point; every
+//    later query is seeded with two real candidate triangles (the previous
+//    closest one and the seed-grid one at x), which bounds the traversal to the
+//    walker's neighbourhood without changing the exact (d2, id) result;
 //  * per-point FP64 sum / sum of squares accumulated per lane over its chunk,
 //    merged across lanes with warp shuffles and flushed with FP64 atomics.
 #include <cuda_runtime.h>
@@ -96,51 +97,268 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   return v;
 }
 
+// Per-lane state of one closest-point query in flight (stack in local memory).
+struct TravState {
+  int sp;
+  int ref;       // inner node to expand next, or kEmptyChild
+  int leaf_cur;  // next triangle slot of the leaf being tested
+  int leaf_end;
+};
+
+// One unit of traversal work for one lane: test ONE triangle of the current
+// leaf, or expand ONE 4-wide node (same ordering and pruning as
+// dev::traverse: children sorted by box distance, nearest entered, others
+// pushed far-to-near, popped entries re-checked).  Returns false once the
+// query is complete.  Splitting the traversal into equal-sized steps is what
+// lets lanes with short queries move on while others are still searching.
+__device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                          dev::V3 p, dev::ClosestHit& hit, TravState& t, int2* stack,
+                                          uint32_t& c_nodes, uint32_t& c_tris, bool& overflow) {
+  if (t.leaf_cur >= t.leaf_end && t.ref == kEmptyChild) {
+    bool found = false;
+    while (t.sp > 0) {
+      const int2 e = stack[--t.sp];
+      if (__int_as_float(e.y) <= hit.d2) {
+        if (e.x >= 0) {
+          t.ref = e.x;
+        } else {
+          t.leaf_cur = leaf_first(e.x);
+          t.leaf_end = t.leaf_cur + leaf_count(e.x);
+        }
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  if (t.leaf_cur < t.leaf_end) {
+    dev::test_slot(tris, t.leaf_cur, p, hit);
+    ++t.leaf_cur;
+    ++c_tris;
+    return true;
+  }
+  const float4* n = nodes + static_cast<size_t>(t.ref) * 8;
+  const float4 lox = __ldg(n + 0);
+  const float4 hix = __ldg(n + 1);
+  const float4 loy = __ldg(n + 2);
+  const float4 hiy = __ldg(n + 3);
+  const float4 loz = __ldg(n + 4);
+  const float4 hiz = __ldg(n + 5);
+  const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
+  ++c_nodes;
+  float d0 = dev::box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
+  float d1 = dev::box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
+  float d2 = dev::box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
+  float d3 = dev::box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
+  int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
+  dev::cswap(d0, r0, d1, r1);
+  dev::cswap(d2, r2, d3, r3);
+  dev::cswap(d0, r0, d2, r2);
+  dev::cswap(d1, r1, d3, r3);
+  dev::cswap(d1, r1, d2, r2);
+  const float best = hit.d2;
+  if (d3 <= best) {
+    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r3, __float_as_int(d3));
+    else overflow = true;
+  }
+  if (d2 <= best) {
+    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r2, __float_as_int(d2));
+    else overflow = true;
+  }
+  if (d1 <= best) {
+    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r1, __float_as_int(d1));
+    else overflow = true;
+  }
+  t.ref = kEmptyChild;
+  if (d0 <= best) {
+    if (r0 >= 0) {
+      t.ref = r0;
+    } else {
+      t.leaf_cur = leaf_first(r0);
+      t.leaf_end = t.leaf_cur + leaf_count(r0);
+    }
+  }
+  return true;
+}
+
+// Persistent walker: a two-phase loop per warp.
+//  Phase A (warp-uniform): finished queries are consumed — the walk stops and
+//    is scored, or moves to its next ball and seeds its next query; finished
+//    chunks are flushed into the per-point FP64 totals; idle lanes pop new
+//    chunks from the global queue.
+//  Phase B: every lane with a query in flight performs traversal steps; the
+//    warp returns to Phase A once `regen` lanes are waiting (or none is busy),
+//    so the walk updates run for many lanes at once and no lane waits for
+//    another lane's whole traversal.
 template <int kOut, int kWalk>
 __global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t t_start = (a.deadline_ns > 0) ? global_ns() : 0;
 
   bool alive = false;     // a walk is in progress on this lane
+  bool querying = false;  // its closest-point query is in flight
   bool exhausted = false; // the global queue has no chunk left for this lane
   int64_t pid = -1;
   int walk = 0, walk_end = 0;
-  dev::V3 x = dev::v3(0, 0, 0), P = dev::v3(0, 0, 0), xm = dev::v3(0, 0, 0);
+  dev::V3 x = dev::v3(0, 0, 0), xm = dev::v3(0, 0, 0);
   float src = 0.0f, am = 0.0f;
   int step = 0, cont0 = 0;
-  bool has_xm = false;
+  bool has_xm = false, w_overflow = false;
   uint64_t wid = 0;
 
-  double acc_s = 0.0, acc_s2 = 0.0;
-  uint32_t acc_n = 0, acc_forced = 0;
-  uint64_t acc_steps = 0;
+  dev::ClosestHit hit;
+  hit.d2 = FLT_MAX;
+  hit.id = INT32_MAX;
+  hit.slot = 0;
+  hit.cp = x;
+  TravState tv{0, kEmptyChild, 0, 0};
+  int2 stack[kTraversalStack];
 
-  unsigned long long c_walks = 0, c_steps = 0, c_queries = 0, c_nodes = 0, c_tris = 0, c_overflow = 0,
-                     c_forced = 0, c_timeout = 0;
+  double acc_s = 0.0, acc_s2 = 0.0;
+  uint32_t acc_n = 0, acc_forced = 0, acc_steps = 0;
+
+  // Per-thread run counters (32-bit; spilled to the 64-bit totals when large).
+  uint32_t c_walks = 0, c_steps = 0, c_queries = 0, c_nodes = 0, c_tris = 0, c_overflow = 0, c_forced = 0,
+           c_timeout = 0;
 
   for (;;) {
+    // ================= Phase A =================
     // (1) deadline: abandon the current walk and stop taking work.
     if (a.deadline_ns > 0 && !exhausted && (global_ns() - t_start) > static_cast<uint64_t>(a.deadline_ns)) {
       if (alive) ++c_timeout;
       alive = false;
+      querying = false;
       exhausted = true;
       walk = walk_end;
     }
-    // (2) flush a finished (or abandoned) chunk's accumulators; always before
-    //     the exit test below, so nothing accumulated is ever dropped.
+    // (2) consume finished queries: score and finish, or move and seed the next
+    //     query.  A finished walk with more walks left in its chunk starts the
+    //     next one at once from the point's cached first query.
+    while (alive && !querying) {
+      ++c_queries;
+      const float d = sqrtf(fmaxf(hit.d2, 0.0f));
+      const int rel = step - cont0;  // steps since the walk (or its continuation) began
+      const bool forced = rel >= a.max_steps;
+      const bool stop = d <= a.eps || forced || !isfinite(d) || hit.id == INT32_MAX;
+      if (stop || (kWalk == N2W_WALK_PREFIX && step >= a.depth_m)) {
+        const float value = stop ? src + problem_u<float>(a.problem, hit.cp.x, hit.cp.y, hit.cp.z) : src;
+        ++c_walks;
+        c_steps += static_cast<uint32_t>(step);
+        c_forced += forced ? 1u : 0u;
+        if (kOut == kOutStats) {
+          acc_s += static_cast<double>(value);
+          acc_s2 += static_cast<double>(value) * static_cast<double>(value);
+          ++acc_n;
+          acc_steps += static_cast<uint32_t>(step);
+          acc_forced += forced ? 1u : 0u;
+        } else {
+          const uint64_t s = wid;
+          if (kOut == kOutSamples) {
+            a.s_value[s] = value;
+          } else {
+            // Prefix outputs (reference cubql_bvh.cu:1451-1606): X is X_m when the
+            // cache is needed, else the position where the walk stopped.
+            const bool needs = (kWalk == N2W_WALK_PREFIX) ? !stop : has_xm;
+            const dev::V3 xo = (kWalk == N2W_WALK_RESIDUAL && has_xm) ? xm : x;
+            a.p_inputs[3 * s + 0] = fminf(1.0f, fmaxf(0.0f, (xo.x - a.in_min[0]) / fmaxf(a.in_ext[0], 1.0e-6f)));
+            a.p_inputs[3 * s + 1] = fminf(1.0f, fmaxf(0.0f, (xo.y - a.in_min[1]) / fmaxf(a.in_ext[1], 1.0e-6f)));
+            a.p_inputs[3 * s + 2] = fminf(1.0f, fmaxf(0.0f, (xo.z - a.in_min[2]) / fmaxf(a.in_ext[2], 1.0e-6f)));
+            a.p_needs[s] = needs ? 1 : 0;
+            if (kWalk == N2W_WALK_PREFIX) {
+              a.p_boundary[s] = value;
+            } else {
+              a.p_boundary[s] = needs ? am : value;
+              a.p_cont[s] = needs ? (value - am) : value;
+            }
+          }
+          a.s_steps[s] = step;
+          a.s_forced[s] = forced ? 1 : 0;
+          a.s_overflow[s] = w_overflow ? 1 : 0;
+        }
+        ++walk;
+        if (walk < walk_end) {
+          // next walk of the same chunk: same point, cached first query
+          const n2w_vec3 p0 = a.points[pid];
+          x = dev::v3(p0.x, p0.y, p0.z);
+          src = 0.0f;
+          step = 0;
+          cont0 = 0;
+          has_xm = false;
+          w_overflow = false;
+          ++wid;
+          const float4 c = __ldg(a.first_cpd + pid);
+          const int2 ii = __ldg(a.first_ids + pid);
+          hit.cp = dev::v3(c.x, c.y, c.z);
+          hit.d2 = c.w;
+          hit.id = ii.x;
+          hit.slot = ii.y;
+        } else {
+          alive = false;
+        }
+        continue;
+      }
+      if (kWalk == N2W_WALK_RESIDUAL && step == a.depth_m && !has_xm) {
+        // X_m reached: remember it and the prefix source; the continuation gets a
+        // fresh max_steps budget like the reference's nc_wos_from_point(X_m).
+        xm = x;
+        am = src;
+        has_xm = true;
+        cont0 = step;
+      }
+      const float R = a.step_scale * d;
+      const U4 r = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                    static_cast<uint32_t>(step), 0u},
+                                 a.k0, a.k1);
+      const dev::V3 dir = unit_sphere(r.x, r.y);
+      if (a.has_source) {
+        float f;
+        if (a.source_center) {
+          f = problem_f<float>(a.problem, x.x, x.y, x.z);
+        } else {
+          const float tfrac = green_radius_fraction(u01(r.z));
+          const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                         static_cast<uint32_t>(step), 1u},
+                                      a.k0, a.k1);
+          const dev::V3 w = unit_sphere(r2.x, r2.y);
+          const float rho = R * tfrac;
+          f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
+        }
+        src += (R * R) * (1.0f / 6.0f) * f;
+      }
+      const int prev_slot = hit.slot;
+      x = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
+      ++step;
+      // Seed the next query with two real candidates (previous closest
+      // triangle, seed-grid triangle at x); the exact answer is unchanged.
+      hit.d2 = FLT_MAX;
+      hit.id = INT32_MAX;
+      hit.cp = x;
+      dev::test_slot(a.tris, prev_slot, x, hit);
+      ++c_tris;
+      if (a.grid.slots) {
+        const int sg = dev::seed_slot(a.grid, x);
+        if (sg != prev_slot) {
+          dev::test_slot(a.tris, sg, x, hit);
+          ++c_tris;
+        }
+      }
+      tv.sp = 0;
+      tv.ref = 0;
+      tv.leaf_cur = tv.leaf_end = 0;
+      querying = true;
+    }
+    // (3) flush finished (or abandoned) chunks' accumulators; always before the
+    //     exit test below, so nothing accumulated is ever dropped.
     if (kOut == kOutStats) {
       const bool want = !alive && walk >= walk_end && acc_n > 0;
       warp_flush(want, pid, acc_s, acc_s2, acc_n, acc_steps, acc_forced, a);
       if (want) {
         acc_s = acc_s2 = 0.0;
-        acc_n = acc_forced = 0;
-        acc_steps = 0;
+        acc_n = acc_forced = acc_steps = 0;
       }
     }
-    // (3) next walk of the current chunk, else pop a new chunk.
-    bool start = false;
-    if (!alive && !exhausted && walk < walk_end) start = true;
-    const bool need = !alive && !exhausted && !start;
+    // (4) pop new chunks for idle lanes (one warp-aggregated atomic).
+    const bool need = !alive && !exhausted;
     const unsigned need_mask = __ballot_sync(0xffffffffu, need);
     if (need_mask) {
       const int leader = __ffs(need_mask) - 1;
@@ -153,156 +371,94 @@ __global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArg
           pid = static_cast<int64_t>(c / static_cast<unsigned long long>(a.chunks_per_point));
           walk = static_cast<int>((c % static_cast<unsigned long long>(a.chunks_per_point)) * a.chunk);
           walk_end = min(walk + a.chunk, a.walks_per_point);
-          start = true;
+          const n2w_vec3 p0 = a.points[pid];
+          x = dev::v3(p0.x, p0.y, p0.z);
+          src = 0.0f;
+          step = 0;
+          cont0 = 0;
+          has_xm = false;
+          w_overflow = false;
+          wid = static_cast<uint64_t>(pid) * static_cast<uint64_t>(a.walks_per_point) + static_cast<uint64_t>(walk);
+          const float4 cc = __ldg(a.first_cpd + pid);
+          const int2 ii = __ldg(a.first_ids + pid);
+          hit.cp = dev::v3(cc.x, cc.y, cc.z);
+          hit.d2 = cc.w;
+          hit.id = ii.x;
+          hit.slot = ii.y;
+          alive = true;  // its (cached) first query is consumed in the next Phase A
         } else {
           exhausted = true;
         }
       }
     }
-    if (start) {
-      const n2w_vec3 p0 = a.points[pid];
-      x = dev::v3(p0.x, p0.y, p0.z);
-      src = 0.0f;
-      step = 0;
-      cont0 = 0;
-      has_xm = false;
-      wid = static_cast<uint64_t>(pid) * static_cast<uint64_t>(a.walks_per_point) + static_cast<uint64_t>(walk);
-      alive = true;
-    }
     if (!__any_sync(0xffffffffu, alive)) break;
-    if (!alive) continue;
 
-    // (4) one closest-point query + one ball move.
-    dev::ClosestHit hit;
-    hit.id = INT32_MAX;
-    hit.cp = x;
-    if (step == 0) {
-      hit.d2 = FLT_MAX;
-    } else {
-      const float dx = x.x - P.x, dy = x.y - P.y, dz = x.z - P.z;
-      const float db = sqrtf(dx * dx + dy * dy + dz * dz) * 1.0001f + 2.0e-6f;
-      hit.d2 = db * db;
-    }
-    dev::TraversalStats st{0, 0, 0};
-    dev::traverse<true>(a.nodes, a.tris, x, hit, st);
-    if (hit.id == INT32_MAX && step > 0) {
-      // The warm bound sat below the numerically computed minimum; redo cold.
-      hit.d2 = FLT_MAX;
-      hit.cp = x;
-      dev::traverse<true>(a.nodes, a.tris, x, hit, st);
-    }
-    ++c_queries;
-    c_nodes += st.node_visits;
-    c_tris += st.tri_tests;
-    c_overflow += st.overflow;
-
-    const float d = sqrtf(fmaxf(hit.d2, 0.0f));
-    const int rel = step - cont0;  // steps since the walk (or its continuation) began
-    const bool forced = rel >= a.max_steps;
-    const bool stop = d <= a.eps || forced || !isfinite(d) || hit.id == INT32_MAX;
-    bool finished = false;
-    float value = 0.0f;
-    if (stop) {
-      value = src + problem_u<float>(a.problem, hit.cp.x, hit.cp.y, hit.cp.z);
-      finished = true;
-    } else if (kWalk == N2W_WALK_PREFIX && step >= a.depth_m) {
-      value = src;
-      finished = true;
-    }
-    if (finished) {
-      ++c_walks;
-      c_steps += static_cast<unsigned long long>(step);
-      c_forced += forced ? 1ull : 0ull;
-      if (kOut == kOutStats) {
-        acc_s += static_cast<double>(value);
-        acc_s2 += static_cast<double>(value) * static_cast<double>(value);
-        ++acc_n;
-        acc_steps += static_cast<uint64_t>(step);
-        acc_forced += forced ? 1u : 0u;
-      } else {
-        const uint64_t s = wid;
-        if (kOut == kOutSamples) {
-          a.s_value[s] = value;
-          a.s_steps[s] = step;
-          a.s_forced[s] = forced ? 1 : 0;
-          a.s_overflow[s] = st.overflow;
-        } else {
-          // Prefix outputs (reference cubql_bvh.cu:1451-1606): X is X_m when the
-          // cache is needed, else the position where the walk stopped.
-          const bool needs = (kWalk == N2W_WALK_PREFIX) ? !stop : has_xm;
-          const dev::V3 xo = (kWalk == N2W_WALK_RESIDUAL && has_xm) ? xm : x;
-          a.p_inputs[3 * s + 0] = fminf(1.0f, fmaxf(0.0f, (xo.x - a.in_min[0]) / fmaxf(a.in_ext[0], 1.0e-6f)));
-          a.p_inputs[3 * s + 1] = fminf(1.0f, fmaxf(0.0f, (xo.y - a.in_min[1]) / fmaxf(a.in_ext[1], 1.0e-6f)));
-          a.p_inputs[3 * s + 2] = fminf(1.0f, fmaxf(0.0f, (xo.z - a.in_min[2]) / fmaxf(a.in_ext[2], 1.0e-6f)));
-          a.p_needs[s] = needs ? 1 : 0;
-          if (kWalk == N2W_WALK_PREFIX) {
-            a.p_boundary[s] = value;
-          } else {
-            a.p_boundary[s] = needs ? am : value;
-            a.p_cont[s] = needs ? (value - am) : value;
-          }
-          a.s_steps[s] = step;
-          a.s_forced[s] = forced ? 1 : 0;
-          a.s_overflow[s] = st.overflow;
+    // ================= Phase B =================
+    for (;;) {
+      const unsigned busy = __ballot_sync(0xffffffffu, querying);
+      const unsigned waiting = __ballot_sync(0xffffffffu, !querying && alive);
+      if (busy == 0 || __popc(waiting) >= a.regen) break;
+      if (querying) {
+        bool ov = false;
+        if (!trav_step(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
+        if (ov) {
+          w_overflow = true;
+          ++c_overflow;
         }
       }
-      alive = false;
-      ++walk;
-      continue;
     }
-
-    if (kWalk == N2W_WALK_RESIDUAL && step == a.depth_m && !has_xm) {
-      // X_m reached: remember it and the prefix source; the continuation gets a
-      // fresh max_steps budget like the reference's nc_wos_from_point(X_m).
-      xm = x;
-      am = src;
-      has_xm = true;
-      cont0 = step;
+    if (a.counters && (c_nodes >= 0x40000000u || c_tris >= 0x40000000u)) {
+      atomicAdd(&a.counters->node_visits, static_cast<unsigned long long>(c_nodes));
+      atomicAdd(&a.counters->tri_tests, static_cast<unsigned long long>(c_tris));
+      c_nodes = c_tris = 0;
     }
-    const float R = a.step_scale * d;
-    const U4 r = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
-                                  static_cast<uint32_t>(step), 0u},
-                               a.k0, a.k1);
-    const dev::V3 dir = unit_sphere(r.x, r.y);
-    if (a.has_source) {
-      float f;
-      if (a.source_center) {
-        f = problem_f<float>(a.problem, x.x, x.y, x.z);
-      } else {
-        const float t = green_radius_fraction(u01(r.z));
-        const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
-                                       static_cast<uint32_t>(step), 1u},
-                                    a.k0, a.k1);
-        const dev::V3 w = unit_sphere(r2.x, r2.y);
-        const float rho = R * t;
-        f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
-      }
-      src += (R * R) * (1.0f / 6.0f) * f;
-    }
-    P = hit.cp;
-    x = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
-    ++step;
   }
 
   if (a.counters) {
-    c_walks = warp_sum_u64(c_walks);
-    c_steps = warp_sum_u64(c_steps);
-    c_queries = warp_sum_u64(c_queries);
-    c_nodes = warp_sum_u64(c_nodes);
-    c_tris = warp_sum_u64(c_tris);
-    c_overflow = warp_sum_u64(c_overflow);
-    c_forced = warp_sum_u64(c_forced);
-    c_timeout = warp_sum_u64(c_timeout);
+    const unsigned long long s_walks = warp_sum_u64(c_walks), s_steps = warp_sum_u64(c_steps),
+                             s_queries = warp_sum_u64(c_queries), s_nodes = warp_sum_u64(c_nodes),
+                             s_tris = warp_sum_u64(c_tris), s_over = warp_sum_u64(c_overflow),
+                             s_forced = warp_sum_u64(c_forced), s_timeout = warp_sum_u64(c_timeout);
     if (lane == 0) {
-      atomicAdd(&a.counters->walks, c_walks);
-      atomicAdd(&a.counters->steps, c_steps);
-      atomicAdd(&a.counters->queries, c_queries);
-      atomicAdd(&a.counters->node_visits, c_nodes);
-      atomicAdd(&a.counters->tri_tests, c_tris);
-      atomicAdd(&a.counters->overflow, c_overflow);
-      atomicAdd(&a.counters->forced, c_forced);
-      atomicAdd(&a.counters->timed_out, c_timeout);
+      atomicAdd(&a.counters->walks, s_walks);
+      atomicAdd(&a.counters->steps, s_steps);
+      atomicAdd(&a.counters->queries, s_queries);
+      atomicAdd(&a.counters->node_visits, s_nodes);
+      atomicAdd(&a.counters->tri_tests, s_tris);
+      atomicAdd(&a.counters->overflow, s_over);
+      atomicAdd(&a.counters->forced, s_forced);
+      atomicAdd(&a.counters->timed_out, s_timeout);
     }
+  }
+}
+
+// ---- per-point first query ----------------------------------------------------
+__global__ void __launch_bounds__(256) first_query_kernel(const float4* __restrict__ nodes,
+                                                          const float4* __restrict__ tris, const dev::SeedGrid grid,
+                                                          const n2w_vec3* __restrict__ points, int64_t n,
+                                                          float4* __restrict__ cpd, int2* __restrict__ ids,
+                                                          n2w_walk_counters* counters) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const n2w_vec3 pt = points[i];
+  const dev::V3 p = dev::v3(pt.x, pt.y, pt.z);
+  dev::ClosestHit hit;
+  hit.d2 = FLT_MAX;
+  hit.id = INT32_MAX;
+  hit.slot = -1;
+  hit.cp = p;
+  dev::TraversalStats st{0, 0, 0};
+  if (grid.slots) {
+    dev::test_slot(tris, dev::seed_slot(grid, p), p, hit);
+    ++st.tri_tests;
+  }
+  dev::traverse<true>(nodes, tris, p, hit, st);
+  cpd[i] = make_float4(hit.cp.x, hit.cp.y, hit.cp.z, hit.d2);
+  ids[i] = make_int2(hit.id, hit.slot);
+  if (counters) {
+    atomicAdd(&counters->node_visits, static_cast<unsigned long long>(st.node_visits));
+    atomicAdd(&counters->tri_tests, static_cast<unsigned long long>(st.tri_tests));
+    if (st.overflow) atomicAdd(&counters->overflow, 1ull);
   }
 }
 
@@ -394,6 +550,7 @@ void validate_walk_options(const n2w_walk_options& o) {
   N2W_REQUIRE(o.block_size == 0 || (o.block_size >= 32 && o.block_size <= kWalkerMaxThreads && o.block_size % 32 == 0),
               "walker block_size must be 0 or a multiple of 32 in [32, 256]");
   N2W_REQUIRE(o.chunk >= 0, "chunk must be non-negative");
+  N2W_REQUIRE(o.regen_threshold >= 0 && o.regen_threshold <= 32, "regen_threshold must be in [0, 32]");
   N2W_REQUIRE(o.blocks_per_sm >= 0, "blocks_per_sm must be non-negative");
 }
 
@@ -414,10 +571,12 @@ WalkArgs make_walk_args(const n2w_bvh& bvh, const n2w_problem& problem, const n2
   WalkArgs a{};
   a.nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
   a.tris = reinterpret_cast<const float4*>(bvh.d_tris);
+  a.grid = seed_grid_of(bvh);
   a.points = d_points;
   a.walks_per_point = o.walks_per_point;
   a.chunk = o.chunk > 0 ? std::min(o.chunk, o.walks_per_point) : std::min(kDefaultChunk, o.walks_per_point);
   a.chunks_per_point = (o.walks_per_point + a.chunk - 1) / a.chunk;
+  a.regen = o.regen_threshold > 0 ? o.regen_threshold : kDefaultRegen;
   a.total_chunks = point_count * a.chunks_per_point;
   a.max_steps = o.max_steps;
   a.depth_m = o.depth_m;
@@ -431,19 +590,37 @@ WalkArgs make_walk_args(const n2w_bvh& bvh, const n2w_problem& problem, const n2
   return a;
 }
 
-void run_walker(WalkArgs& a, int out_kind, int walk_mode, const n2w_walk_options& o, n2w_walk_counters* d_counters,
-                void* d_workspace, cudaStream_t stream) {
+// Workspace layout: [0, 8) queue counter, [256, 320) run counters when the
+// caller passes none, [512, 512 + 16 n) first-query points+d2 (float4),
+// then 8 n bytes of first-query (id, slot) pairs.
+constexpr size_t kWsHeader = 512;
+
+void run_walker(WalkArgs& a, int64_t point_count, int out_kind, int walk_mode, const n2w_walk_options& o,
+                n2w_walk_counters* d_counters, void* d_workspace, cudaStream_t stream) {
   if (a.total_chunks == 0) return;
+  const size_t ws_bytes = n2w_wos_workspace_bytes(point_count);
   void* ws = d_workspace;
   bool own = false;
   if (!ws) {
-    N2W_CUDA(cudaMallocAsync(&ws, n2w_wos_workspace_bytes(), stream));
+    N2W_CUDA(cudaMallocAsync(&ws, ws_bytes, stream));
     own = true;
   }
-  N2W_CUDA(cudaMemsetAsync(ws, 0, n2w_wos_workspace_bytes(), stream));
-  a.queue = reinterpret_cast<unsigned long long*>(ws);
-  a.counters = d_counters ? d_counters : reinterpret_cast<n2w_walk_counters*>(reinterpret_cast<char*>(ws) + 256);
+  char* base = reinterpret_cast<char*>(ws);
+  N2W_CUDA(cudaMemsetAsync(ws, 0, kWsHeader, stream));
+  a.queue = reinterpret_cast<unsigned long long*>(base);
+  a.counters = d_counters ? d_counters : reinterpret_cast<n2w_walk_counters*>(base + 256);
   if (d_counters) N2W_CUDA(cudaMemsetAsync(d_counters, 0, sizeof(n2w_walk_counters), stream));
+  float4* cpd = reinterpret_cast<float4*>(base + kWsHeader);
+  int2* ids = reinterpret_cast<int2*>(base + kWsHeader + 16 * static_cast<size_t>(point_count));
+  a.first_cpd = cpd;
+  a.first_ids = ids;
+  {
+    const int block = 256;
+    const int64_t grid = (point_count + block - 1) / block;
+    first_query_kernel<<<static_cast<unsigned>(grid), block, 0, stream>>>(a.nodes, a.tris, a.grid, a.points,
+                                                                          point_count, cpd, ids, a.counters);
+    N2W_CUDA(cudaGetLastError());
+  }
   const int block = o.block_size > 0 ? o.block_size : kDefaultWalkerThreads;
   if (out_kind == kOutStats) launch_walker<kOutStats, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
   else if (out_kind == kOutSamples) launch_walker<kOutSamples, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
@@ -466,7 +643,9 @@ using namespace n2w;
 
 extern "C" {
 
-size_t n2w_wos_workspace_bytes(void) { return 512; }
+size_t n2w_wos_workspace_bytes(int64_t point_count) {
+  return kWsHeader + 24 * static_cast<size_t>(point_count < 0 ? 0 : point_count);
+}
 
 int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
                      int64_t point_count, const n2w_walk_options* options, n2w_point_stats stats,
@@ -486,7 +665,7 @@ int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_v
     a.count = stats.d_count;
     a.steps = stats.d_steps;
     a.forced = stats.d_forced;
-    run_walker(a, kOutStats, N2W_WALK_PURE, *options, d_counters, d_workspace, stream);
+    run_walker(a, point_count, kOutStats, N2W_WALK_PURE, *options, d_counters, d_workspace, stream);
   });
 }
 
@@ -507,7 +686,7 @@ int n2w_wos_pure_samples(const n2w_bvh* bvh, const n2w_problem* problem, const n
     a.s_steps = d_step_count;
     a.s_forced = d_forced_max_steps;
     a.s_overflow = d_query_overflow;
-    run_walker(a, kOutSamples, N2W_WALK_PURE, *options, nullptr, nullptr, stream);
+    run_walker(a, point_count, kOutSamples, N2W_WALK_PURE, *options, nullptr, nullptr, stream);
   });
 }
 
@@ -542,7 +721,7 @@ int n2w_wos_prefix_samples(const n2w_bvh* bvh, const n2w_problem* problem,
     a.s_steps = d_step_count;
     a.s_forced = d_forced_max_steps;
     a.s_overflow = d_query_overflow;
-    run_walker(a, kOutPrefix, mode, *options, nullptr, nullptr, stream);
+    run_walker(a, point_count, kOutPrefix, mode, *options, nullptr, nullptr, stream);
   });
 }
 

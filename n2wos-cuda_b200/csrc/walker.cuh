@@ -3,6 +3,7 @@
 
 #include <stdint.h>
 
+#include "geom.cuh"
 #include "n2w.h"
 
 namespace n2w {
@@ -14,15 +15,22 @@ constexpr int kOutPrefix = 2;   // per-sample prefix records for the cache level
 constexpr int kWalkerMaxThreads = 256;
 constexpr int kDefaultWalkerThreads = 128;
 constexpr int kDefaultChunk = 8;
+constexpr int kDefaultRegen = 12;
 
 struct WalkArgs {
   const float4* nodes;
   const float4* tris;
+  dev::SeedGrid grid;
   const n2w_vec3* points;
+  // Per-point first query (closest point + d2, id + slot): every walk of a
+  // point starts with the same query, computed once by a pre-pass.
+  const float4* first_cpd;
+  const int2* first_ids;
   int64_t total_chunks;
   int64_t chunks_per_point;
   int walks_per_point;
   int chunk;
+  int regen;  // waiting lanes that trigger the walk-update phase
   int max_steps;
   int depth_m;
   float eps;
@@ -53,5 +61,7 @@ struct WalkArgs {
   unsigned long long* queue;
   n2w_walk_counters* counters;
 };
+
+dev::SeedGrid seed_grid_of(const n2w_bvh& b);
 
 }  // namespace n2w

@@ -276,6 +276,16 @@ class Bvh:
         call("n2w_bvh_copy_layout", self._h, _ptr(nodes), _ptr(tris))
         return nodes, tris
 
+    def seed_grid(self):
+        """(slots int32[(n+1)^3], lo float32[3], h, n) of the BVH's seed grid."""
+        lo = np.empty(3, np.float32)
+        h = C.c_float()
+        n = C.c_int()
+        call("n2w_bvh_seed_grid", self._h, _ptr(lo), C.byref(h), C.byref(n), None)
+        slots = np.empty((n.value + 1) ** 3, np.int32)
+        call("n2w_bvh_seed_grid", self._h, None, None, None, _ptr(slots))
+        return slots, lo, float(h.value), n.value
+
     def inside(self, points: np.ndarray, block_size: int = 128) -> np.ndarray:
         """Ray-parity inside/outside of each point (uint8 0/1) on the device."""
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
@@ -353,12 +363,13 @@ def problem_eval_f32(p: Problem, xyz: np.ndarray):
 
 
 def walk_options(walks_per_point=256, max_steps=256, depth_m=8, epsilon=1e-3, step_scale=0.999,
-                 seed=12345, block_size=0, blocks_per_sm=0, chunk=0, accumulate=0, deadline_ns=0):
+                 seed=12345, block_size=0, blocks_per_sm=0, chunk=0, accumulate=0, deadline_ns=0,
+                 regen_threshold=0):
     o = WalkOptions()
     o.walks_per_point, o.max_steps, o.depth_m = walks_per_point, max_steps, depth_m
     o.epsilon, o.step_scale, o.seed = epsilon, step_scale, seed
     o.block_size, o.blocks_per_sm, o.chunk = block_size, blocks_per_sm, chunk
-    o.accumulate, o.deadline_ns = accumulate, deadline_ns
+    o.accumulate, o.deadline_ns, o.regen_threshold = accumulate, deadline_ns, regen_threshold
     return o
 
 

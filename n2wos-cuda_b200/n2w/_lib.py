@@ -61,7 +61,7 @@ class WalkOptions(C.Structure):
     _fields_ = [("walks_per_point", C.c_int32), ("max_steps", C.c_int32), ("depth_m", C.c_int32),
                 ("epsilon", C.c_float), ("step_scale", C.c_float), ("seed", C.c_uint64),
                 ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk", C.c_int32),
-                ("accumulate", C.c_int32), ("deadline_ns", C.c_int64)]
+                ("accumulate", C.c_int32), ("deadline_ns", C.c_int64), ("regen_threshold", C.c_int32)]
 
 
 class PointStats(C.Structure):
@@ -118,7 +118,8 @@ _SIGS = {
     "n2w_problem_mode_from_name": (I, [C.c_char_p, C.POINTER(I)]),
     "n2w_problem_mode_name": (C.c_char_p, [I]),
     "n2w_rng_philox4x32_10": (I, [P, C.c_uint64, C.c_uint32, P]),
-    "n2w_wos_workspace_bytes": (C.c_size_t, []),
+    "n2w_wos_workspace_bytes": (C.c_size_t, [I64]),
+    "n2w_bvh_seed_grid": (I, [P, P, P, P, P]),
     "n2w_wos_estimate": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), PointStats, P, P, P]),
     "n2w_wos_pure_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), P, P, P, P, P]),
     "n2w_wos_prefix_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), I, P, P,

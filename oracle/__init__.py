@@ -150,7 +150,8 @@ def _setup():
     L.oracle_bruteforce.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     L.oracle_traverse4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
-                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_float, C.c_int]
     L.oracle_philox4x32_10.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
     L.oracle_closest_point_on_triangle.argtypes = [C.c_void_p] * 5
     L.oracle_wos.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
@@ -174,8 +175,10 @@ def bruteforce(vertices, triangles, points, threads=8):
     return {"distance2": d2, "closest": cp, "triangle_id": ids, "ties": ties}
 
 
-def traverse4(nodes, tris, points, threads=8):
-    """The product's 4-wide traversal restated on the CPU (visit counts)."""
+def traverse4(nodes, tris, points, threads=8, seed=None):
+    """The product's 4-wide traversal restated on the CPU (visit counts).
+
+    seed: optional (slots int32[(n+1)^3], lo float32[3], h, n) seed grid."""
     L = _setup()
     pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
     n = len(pts)
@@ -184,8 +187,16 @@ def traverse4(nodes, tris, points, threads=8):
     ids = np.empty(n, np.int32)
     nv = np.empty(n, np.int32)
     nt = np.empty(n, np.int32)
+    if seed is not None:
+        slots, lo, h, sn = seed
+        slots = np.ascontiguousarray(slots, np.int32)
+        lo = np.ascontiguousarray(lo, np.float32)
+        inv_h = float(np.float32(1.0) / np.float32(h))
+        sargs = (_p(slots), _p(lo), inv_h, int(sn))
+    else:
+        sargs = (None, None, 0.0, 0)
     L.oracle_traverse4(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(tris)), _p(pts), n, _p(d2),
-                       _p(cp), _p(ids), _p(nv), _p(nt), threads)
+                       _p(cp), _p(ids), _p(nv), _p(nt), threads, *sargs)
     return {"distance2": d2, "closest": cp, "triangle_id": ids, "node_visits": nv, "tri_tests": nt}
 
 

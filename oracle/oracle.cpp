@@ -303,13 +303,36 @@ void oracle_bruteforce(const float* verts, const uint32_t* tris, int64_t nt, con
 }
 
 // Restated 4-wide traversal over the product layout (nodes 128 B, tris 48 B).
+// When seed_slots is given, the triangle stored at the nearest seed-grid node
+// (lattice lo + i/inv_h, n cells per axis) is tested first, as the kernel does.
 void oracle_traverse4(const void* nodes, const void* tris, const float* points, int64_t n, float* out_d2,
-                      float* out_cp, int32_t* out_id, int32_t* out_nodes, int32_t* out_tris, int threads) {
+                      float* out_cp, int32_t* out_id, int32_t* out_nodes, int32_t* out_tris, int threads,
+                      const int32_t* seed_slots, const float* seed_lo, float seed_inv_h, int seed_n) {
   const Node4* nd = static_cast<const Node4*>(nodes);
   const TriRec* tr = static_cast<const TriRec*>(tris);
   parallel_for(n, threads, [&](int64_t q) {
     Hit h{FLT_MAX, INT32_MAX, {0, 0, 0}, 0, 0, 0};
-    traverse4(nd, tr, {points[3 * q], points[3 * q + 1], points[3 * q + 2]}, h);
+    const V p{points[3 * q], points[3 * q + 1], points[3 * q + 2]};
+    if (seed_slots) {
+      auto idx = [&](float c, float lo) {
+        const float f = (c - lo) * seed_inv_h;
+        return static_cast<int64_t>(std::nearbyint(std::fmin(std::fmax(f, 0.0f), static_cast<float>(seed_n))));
+      };
+      const int64_t s = seed_n + 1;
+      const int32_t slot = seed_slots[(idx(p.z, seed_lo[2]) * s + idx(p.y, seed_lo[1])) * s + idx(p.x, seed_lo[0])];
+      const TriRec& t = tr[slot];
+      ++h.tris;
+      const V cp = closest_on_triangle(p, {t.v0[0], t.v0[1], t.v0[2]}, {t.v1[0], t.v1[1], t.v1[2]},
+                                       {t.v2[0], t.v2[1], t.v2[2]});
+      const V dv = sub(cp, p);
+      const float dd = dot(dv, dv);
+      if (dd < h.d2 || (dd == h.d2 && t.id < h.id)) {
+        h.d2 = dd;
+        h.id = t.id;
+        h.cp = cp;
+      }
+    }
+    traverse4(nd, tr, p, h);
     out_d2[q] = h.d2;
     out_cp[3 * q] = h.cp.x;
     out_cp[3 * q + 1] = h.cp.y;

@@ -67,6 +67,21 @@ def test_traversal_equals_bruteforce(n2w, bumpy_ref_mesh, golden_closest, method
     assert np.array_equal(tr["triangle_id"], bf["triangle_id"])
 
 
+def test_seeded_traversal_is_exact_for_any_seed(n2w, bumpy_ref_mesh, golden_closest):
+    """Seeds are real candidate triangles: whatever they are, the answer is the
+    brute-force (d2, lowest id) minimum."""
+    v, t = bumpy_ref_mesh.arrays()
+    nodes, tris = n2w.HostBvh(bumpy_ref_mesh, 4, "sah").layout()
+    n = 16
+    slots = np.random.default_rng(5).integers(0, len(tris), (n + 1) ** 3).astype(np.int32)
+    seed = (slots, np.array([-1.3, -1.3, -1.3], np.float32), 2.6 / n, n)
+    pts = golden_closest["points"]
+    tr = oracle.traverse4(nodes, tris, pts, seed=seed)
+    bf = oracle.bruteforce(v, t, pts)
+    assert np.array_equal(tr["distance2"].view(np.uint32), bf["distance2"].view(np.uint32))
+    assert np.array_equal(tr["triangle_id"], bf["triangle_id"])
+
+
 def test_degenerate_and_duplicate_triangles(n2w):
     # A tetrahedron plus a duplicated face and a zero-area sliver.
     v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0, 0]], np.float32)

@@ -42,7 +42,7 @@ def test_config0_queries_vs_oracle(gpu, method, leaf):
     pts = uniform_box(262144, 1.2, 12345)
     r = bvh.query(pts, counted=True)
     nodes, tris = bvh.layout()
-    tr = oracle.traverse4(nodes, tris, pts)
+    tr = oracle.traverse4(nodes, tris, pts, seed=bvh.seed_grid())
     assert_bitexact(r, tr)
     assert np.array_equal(r["node_visits"], tr["node_visits"])
     assert np.array_equal(r["tri_tests"], tr["tri_tests"])
@@ -50,6 +50,19 @@ def test_config0_queries_vs_oracle(gpu, method, leaf):
     sub = {k: r[k][:2048] for k in ("distance2", "closest", "triangle_id")}
     assert_bitexact(sub, bf)
     print(f"ties among 2048 validation points: {(bf['ties'] > 1).sum()}")
+
+
+def test_seed_grid_holds_nearest_triangles(gpu, ref_bvh, bumpy_ref_mesh):
+    slots, lo, h, n = ref_bvh.seed_grid()
+    assert n == 128 and len(slots) == 129 ** 3
+    nodes, tris = ref_bvh.layout()
+    v, t = bumpy_ref_mesh.arrays()
+    idx = np.random.default_rng(3).integers(0, len(slots), 3000)
+    s = n + 1
+    g = np.stack([idx % s, (idx // s) % s, idx // (s * s)], 1).astype(np.float32)
+    pts = (lo + np.float32(h) * g).astype(np.float32)
+    bf = oracle.bruteforce(v, t, pts)
+    assert np.array_equal(tris["id"][slots[idx]], bf["triangle_id"])
 
 
 def test_query_modes_surface_and_shell(gpu):
