@@ -265,6 +265,26 @@ int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_v
                      n2w_point_stats stats, n2w_walk_counters* d_counters, void* d_workspace,
                      n2w_stream_t stream);
 
+/* Allocation-free n2w_wos_estimate.  No counterpart in the reference.
+ * For callers that may not allocate device memory while they solve (a host
+ * application that hands the library a fixed share of HBM and forbids other
+ * allocations; a serving loop that must not call cudaMalloc on its request
+ * path, since cudaMalloc can synchronise the device).  The walker scratch lives
+ * in one static device array of N2W_NOALLOC_SCRATCH_BYTES (4 MiB), held by every
+ * GPU that loads the library until exit; point_count above N2W_NOALLOC_MAX_POINTS
+ * returns N2W_EINVAL.  The caller still passes points and outputs.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current): make that first call before any stream capture.
+ * All calls on a device share the one array, so calls that overlap on the GPU
+ * (other streams, other threads) race: serialise them.  No cudaMalloc /
+ * cudaFree or other allocating routine is called. */
+#define N2W_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define N2W_NOALLOC_MAX_POINTS ((N2W_NOALLOC_SCRATCH_BYTES - 512u) / 24u)
+int n2w_wos_estimate_noalloc(const n2w_bvh* bvh, const n2w_problem* problem,
+                             const n2w_vec3* d_points, int64_t point_count,
+                             const n2w_walk_options* options, n2w_point_stats stats,
+                             n2w_walk_counters* d_counters, n2w_stream_t stream);
+
 /* Per-sample outputs, mirroring launch_nc_pure_wos_samples
  * (include/n2wos/tcnn_nc_wos.hpp:87-93): sample j of point i is at i*W+j. */
 int n2w_wos_pure_samples(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,

@@ -669,6 +669,64 @@ int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_v
   });
 }
 
+}  // extern "C"
+
+// ---- allocation-free variant of n2w_wos_estimate ----------------------------
+// Some callers cannot allocate device memory while they solve: applications
+// that give the library a fixed share of HBM up front and forbid it any other
+// allocation, and serving loops that must never call cudaMalloc or
+// cudaMallocAsync on the request path (cudaMalloc can synchronise the device
+// and stall every stream).  For them, the walker's scratch (queue counter, run
+// counters, each point's cached first query) lives in this static device
+// array.  Every GPU that loads the library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[N2W_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// In host code the array's name is only a host-side stand-in; its device
+// address is looked up once per device, with that device current, and reused.
+void* noalloc_scratch_current_device() {
+  int dev = 0;
+  N2W_CUDA(cudaGetDevice(&dev));
+  N2W_REQUIRE(dev >= 0 && dev < kNoallocMaxDevices, "device index beyond the allocation-free scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      throw Error(N2W_ECUDA, std::string("cudaGetSymbolAddress for the allocation-free scratch failed: ") +
+                                 cudaGetErrorString(e));
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+int n2w_wos_estimate_noalloc(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
+                             int64_t point_count, const n2w_walk_options* options, n2w_point_stats stats,
+                             n2w_walk_counters* d_counters, n2w_stream_t stream) {
+  void* scratch = nullptr;
+  const int st = guarded([&] {
+    N2W_REQUIRE(point_count <= static_cast<int64_t>(N2W_NOALLOC_MAX_POINTS),
+                "n2w_wos_estimate_noalloc: " + std::to_string(point_count) + " points exceed the limit of " +
+                    std::to_string(N2W_NOALLOC_MAX_POINTS) + " points of the static " +
+                    std::to_string(N2W_NOALLOC_SCRATCH_BYTES) +
+                    "-byte scratch; split the points or call n2w_wos_estimate with a workspace");
+    scratch = noalloc_scratch_current_device();
+  });
+  if (st != N2W_OK) return st;
+  // The scratch is passed as the caller workspace, so nothing is allocated.
+  return n2w_wos_estimate(bvh, problem, d_points, point_count, options, stats, d_counters, scratch, stream);
+}
+
 int n2w_wos_pure_samples(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points,
                          int64_t point_count, const n2w_walk_options* options,
                          float* d_sample_values, int* d_step_count, int* d_forced_max_steps,

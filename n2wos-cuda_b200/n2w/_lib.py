@@ -121,6 +121,7 @@ _SIGS = {
     "n2w_wos_workspace_bytes": (C.c_size_t, [I64]),
     "n2w_bvh_seed_grid": (I, [P, P, P, P, P]),
     "n2w_wos_estimate": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), PointStats, P, P, P]),
+    "n2w_wos_estimate_noalloc": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), PointStats, P, P]),
     "n2w_wos_pure_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), P, P, P, P, P]),
     "n2w_wos_prefix_samples": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(WalkOptions), I, P, P,
                                    P, P, P, P, P, P, P, P]),
