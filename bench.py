@@ -62,6 +62,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def traffic_per_walk_step():
+    """DRAM bytes per walk-step of walker_kernel from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of a small capture divided by
+    its walk-steps; traffic grows in proportion to walk-steps)."""
+    p = ROOT / "profiles" / "walker_kernel_icosphere_slice_4096pts.md"
+    if p.exists():
+        for line in p.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_walk_step:"):
+                return float(line.split(":")[1])
+    return None
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -333,7 +345,10 @@ def main():
             "e2e": {"value": e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                     "d2h_bytes_per_step": int(out_bytes)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "frac": achieved / peak,
+                         "traffic": (traffic_per_walk_step() * c_last["steps"]) if traffic_per_walk_step() else None,
+                         "traffic_source": "profiles/walker_kernel_icosphere_slice_4096pts.md (scaled by walk-steps)",
+                         "peak_source": peak_kind,
                          "kernel": "walker_kernel", "bytes_per_launch": alg_bytes,
                          "kernel_ms": kernel_ms},
             "cpu_baseline": cpu,

@@ -320,6 +320,54 @@ int n2w_reduce_samples(const float* d_values, const int* d_step_count, const int
                        int64_t point_count, int walks_per_point, n2w_point_stats stats,
                        int accumulate, n2w_stream_t stream);
 
+/* ---- neural cache (hash grid + MLP), replaces the reference's tiny-cuda-nn
+ *      HashGrid + FullyFusedMLP + Adam (src/tools/eval_tcnn_nc_wos.cu:747-759) -- */
+typedef struct n2w_cache n2w_cache;
+typedef struct n2w_cache_config {
+  int32_t n_levels;             /* 1..16 */
+  int32_t n_features_per_level; /* 2 */
+  int32_t log2_hashmap_size;    /* T = 2^log2 entries per hashed level */
+  float base_resolution;        /* N_min */
+  float per_level_scale;        /* b; 0 = derive from max_resolution */
+  float max_resolution;         /* N_max (used when per_level_scale == 0) */
+  int32_t n_neurons;            /* 16, 32 or 64 */
+  int32_t n_hidden_layers;      /* 1..4 */
+  float learning_rate;          /* Adam */
+  float beta1, beta2, epsilon;
+  uint64_t seed;                /* parameter initialisation */
+} n2w_cache_config;
+
+/* 16 levels x 2 features, 2^19 entries, resolutions 16..2048, 64 x 2 hidden,
+ * Adam lr 1e-2, beta (0.9, 0.99), eps 1e-15. */
+int n2w_cache_config_default(n2w_cache_config* out);
+/* Host-only: parameter counts and per-level resolution / table size of a config. */
+int n2w_cache_describe(const n2w_cache_config* cfg, int64_t* grid_params, int64_t* mlp_params,
+                       int32_t* level_resolution, int32_t* level_table_size);
+int n2w_cache_create(const n2w_cache_config* cfg, n2w_cache** out);
+void n2w_cache_destroy(n2w_cache* cache);
+/* Parameter counts (floats) and per-level resolution / table size (arrays of n_levels). */
+int n2w_cache_info(const n2w_cache* cache, n2w_cache_config* cfg_out, int64_t* grid_params,
+                   int64_t* mlp_params, int32_t* level_resolution, int32_t* level_table_size);
+/* C(x) for n inputs in the unit cube (float[3n]) -> d_outputs[n]. */
+int n2w_cache_infer(const n2w_cache* cache, const float* d_inputs, int64_t n, float* d_outputs,
+                    n2w_stream_t stream);
+/* Adds d(mean (C(x)-t)^2)/d(params) into the cache's gradient buffer (no update);
+ * d_outputs (may be NULL) receives C(x).  Used by gradient checks. */
+int n2w_cache_gradients(n2w_cache* cache, const float* d_inputs, const float* d_targets, int64_t n,
+                        float* d_outputs, n2w_stream_t stream);
+/* One Adam step on the L2 loss mean (C(x)-t)^2 over the batch; *h_loss_out (may be
+ * NULL; synchronises when given) receives the batch loss before the update. */
+int n2w_cache_train_step(n2w_cache* cache, const float* d_inputs, const float* d_targets, int64_t n,
+                         float* h_loss_out, n2w_stream_t stream);
+int n2w_cache_zero_grad(n2w_cache* cache, n2w_stream_t stream);
+/* Host copies of the FP32 master parameters, the FP16 working copy and the FP32
+ * gradient ([grid | mlp] order; any pointer may be NULL). */
+int n2w_cache_get_params(const n2w_cache* cache, float* h_fp32, uint16_t* h_fp16, float* h_grad);
+int n2w_cache_set_params(n2w_cache* cache, const float* h_fp32);
+/* Versioned binary checkpoint: config, step, parameters, Adam moments. */
+int n2w_cache_save(const n2w_cache* cache, const char* path);
+int n2w_cache_load(const char* path, n2w_cache** out);
+
 /* ---- thin device-memory helpers for callers without a CUDA binding ------ */
 int n2w_device_count(int* out);
 int n2w_set_device(int device);

@@ -430,6 +430,109 @@ def wos_estimate(bvh: Bvh, problem: Problem, points: np.ndarray | DeviceBuffer, 
     return res, cnt
 
 
+def cache_config(**overrides):
+    """Default cache config (16 levels x 2, 2^19, res 16..2048, 64x2 hidden, Adam 1e-2)."""
+    from ._lib import CacheConfig
+
+    cfg = CacheConfig()
+    call("n2w_cache_config_default", C.byref(cfg))
+    for k, v in overrides.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def cache_describe(cfg):
+    g, m = C.c_int64(), C.c_int64()
+    res = np.zeros(16, np.int32)
+    tab = np.zeros(16, np.int32)
+    call("n2w_cache_describe", C.byref(cfg), C.byref(g), C.byref(m), _ptr(res), _ptr(tab))
+    L = cfg.n_levels
+    return {"grid_params": g.value, "mlp_params": m.value, "resolution": res[:L].copy(), "table_size": tab[:L].copy()}
+
+
+class Cache:
+    """Hash-grid + MLP neural cache on the device (replaces tiny-cuda-nn)."""
+
+    def __init__(self, cfg=None, handle=None):
+        if handle is not None:
+            self._h = handle
+        else:
+            cfg = cfg or cache_config()
+            self._h = C.c_void_p()
+            call("n2w_cache_create", C.byref(cfg), C.byref(self._h))
+
+    @classmethod
+    def load(cls, path: str) -> "Cache":
+        h = C.c_void_p()
+        call("n2w_cache_load", str(path).encode(), C.byref(h))
+        return cls(handle=h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        from ._lib import CacheConfig
+
+        cfg = CacheConfig()
+        g, m = C.c_int64(), C.c_int64()
+        res = np.zeros(16, np.int32)
+        tab = np.zeros(16, np.int32)
+        call("n2w_cache_info", self._h, C.byref(cfg), C.byref(g), C.byref(m), _ptr(res), _ptr(tab))
+        L = cfg.n_levels
+        return {"config": cfg, "grid_params": g.value, "mlp_params": m.value, "resolution": res[:L].copy(),
+                "table_size": tab[:L].copy()}
+
+    def n_params(self) -> int:
+        i = self.info()
+        return i["grid_params"] + i["mlp_params"]
+
+    def params(self):
+        n = self.n_params()
+        p32 = np.empty(n, np.float32)
+        p16 = np.empty(n, np.uint16)
+        g = np.empty(n, np.float32)
+        call("n2w_cache_get_params", self._h, _ptr(p32), _ptr(p16), _ptr(g))
+        return p32, p16.view(np.float16), g
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert len(p) == self.n_params()
+        call("n2w_cache_set_params", self._h, _ptr(p))
+
+    def infer(self, inputs: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(inputs, np.float32).reshape(-1, 3)
+        n = len(x)
+        dx = DeviceBuffer.from_array(x)
+        dy = DeviceBuffer(4 * max(n, 1))
+        call("n2w_cache_infer", self._h, dx.ptr, n, dy.ptr, None)
+        return dy.download(np.float32, n)
+
+    def gradients(self, inputs, targets):
+        x = np.ascontiguousarray(inputs, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(targets, np.float32)
+        dx, dt = DeviceBuffer.from_array(x), DeviceBuffer.from_array(t)
+        dy = DeviceBuffer(4 * len(x))
+        call("n2w_cache_zero_grad", self._h, None)
+        call("n2w_cache_gradients", self._h, dx.ptr, dt.ptr, len(x), dy.ptr, None)
+        call("n2w_device_sync")
+        return dy.download(np.float32, len(x)), self.params()[2]
+
+    def train_step(self, d_inputs, d_targets, n, stream=None) -> float:
+        loss = C.c_float()
+        call("n2w_cache_train_step", self._h, d_inputs, d_targets, n, C.byref(loss),
+             stream.handle if stream else None)
+        return float(loss.value)
+
+    def save(self, path: str):
+        call("n2w_cache_save", self._h, str(path).encode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.n2w_cache_destroy(self._h)
+            self._h = None
+
+
 def device_count() -> int:
     n = C.c_int()
     st = lib.n2w_device_count(C.byref(n))

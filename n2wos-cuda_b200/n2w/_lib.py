@@ -75,6 +75,13 @@ class WalkCounters(C.Structure):
                  "timed_out")]
 
 
+class CacheConfig(C.Structure):
+    _fields_ = [("n_levels", C.c_int32), ("n_features_per_level", C.c_int32), ("log2_hashmap_size", C.c_int32),
+                ("base_resolution", C.c_float), ("per_level_scale", C.c_float), ("max_resolution", C.c_float),
+                ("n_neurons", C.c_int32), ("n_hidden_layers", C.c_int32), ("learning_rate", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float), ("seed", C.c_uint64)]
+
+
 P = C.c_void_p
 I = C.c_int
 I64 = C.c_int64
@@ -127,6 +134,19 @@ _SIGS = {
                                    P, P, P, P, P, P, P, P]),
     "n2w_wos_combine": (I, [P, P, P, P, I64, P, P, I, P]),
     "n2w_reduce_samples": (I, [P, P, P, I64, I, PointStats, I, P]),
+    "n2w_cache_config_default": (I, [C.POINTER(CacheConfig)]),
+    "n2w_cache_describe": (I, [C.POINTER(CacheConfig), C.POINTER(I64), C.POINTER(I64), P, P]),
+    "n2w_cache_create": (I, [C.POINTER(CacheConfig), PP]),
+    "n2w_cache_destroy": (None, [P]),
+    "n2w_cache_info": (I, [P, C.POINTER(CacheConfig), C.POINTER(I64), C.POINTER(I64), P, P]),
+    "n2w_cache_infer": (I, [P, P, I64, P, P]),
+    "n2w_cache_gradients": (I, [P, P, P, I64, P, P]),
+    "n2w_cache_train_step": (I, [P, P, P, I64, C.POINTER(C.c_float), P]),
+    "n2w_cache_zero_grad": (I, [P, P]),
+    "n2w_cache_get_params": (I, [P, P, P, P]),
+    "n2w_cache_set_params": (I, [P, P]),
+    "n2w_cache_save": (I, [P, C.c_char_p]),
+    "n2w_cache_load": (I, [C.c_char_p, PP]),
     "n2w_device_count": (I, [C.POINTER(I)]),
     "n2w_set_device": (I, [I]),
     "n2w_malloc": (I, [PP, C.c_size_t]),
