@@ -141,12 +141,14 @@ def cpu_port_sample(n2w, bvh_or_layout, problem, pts, walks, seconds_target=12.0
 
     nodes, tris = bvh_or_layout
     threads = threads or os.cpu_count() or 1
-    # calibration on a few points, then a sample sized for ~seconds_target
+    # calibration on an evenly spread set of points (walk cost depends on the
+    # distance to the boundary), then a sample sized for ~seconds_target
+    cal = pts[np.linspace(0, len(pts) - 1, max(64, 4 * threads)).astype(np.int64)]
     t0 = time.perf_counter()
-    r = oracle.wos(nodes, tris, bytes(problem), pts[:threads], walks, 256, 5e-4, 0.999, 12345, 0, threads)
+    oracle.wos(nodes, tris, bytes(problem), cal, walks, 256, 5e-4, 0.999, 12345, 0, threads)
     dt = time.perf_counter() - t0
-    per_point = max(dt, 1e-6) / max(1, min(threads, len(pts)))
-    n = int(np.clip(seconds_target / per_point * threads, threads, len(pts)))
+    per_point = max(dt, 1e-6) / len(cal)  # wall seconds per point with all threads busy
+    n = int(np.clip(seconds_target / per_point, threads, len(pts)))
     sel = pts[np.linspace(0, len(pts) - 1, n).astype(np.int64)]
     t0 = time.perf_counter()
     r = oracle.wos(nodes, tris, bytes(problem), sel, walks, 256, 5e-4, 0.999, 12345, 0, threads)
@@ -154,6 +156,89 @@ def cpu_port_sample(n2w, bvh_or_layout, problem, pts, walks, seconds_target=12.0
     steps = float(r["steps"].sum())
     return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} of {len(pts)} slice points x {walks} walks ({steps:.3g} walk-steps) in {dt:.1f} s"}
+
+
+def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub=16384, train_steps=200):
+    """Time for the slice MSE against the FP64 analytic u to reach `target`:
+    plain GPU WoS vs NC+2LMC (cache trained online from WoS labels, coarse walks
+    truncated at depth 8 and closed by the cache, unbiased residual from 1/16 of
+    the walks).  Per-walk cost and variance are measured on the device for an
+    evenly spaced subsample of the slice; MSE(N) = bias^2 + var/N is extrapolated
+    to the full slice (the estimator is unbiased, so the target is reached at
+    N = var / (target - bias^2))."""
+    from n2w import nc
+
+    P = len(pts)
+    sel = np.linspace(0, P - 1, min(sub, P)).astype(np.int64)
+    x, ex = np.ascontiguousarray(pts[sel]), exact[sel]
+    n = len(x)
+    dp = n2w.DeviceBuffer.from_array(x)
+    t = n2w.Timer()
+    st = n2w.PointStatsBuffers.allocate(n)
+    ws = n2w.DeviceBuffer(lib.n2w_wos_workspace_bytes(n))
+    W = 256
+    out = {"target_mse": target, "subsample_points": n, "slice_points": P, "walks_measured_per_point": W}
+
+    def plain(pb):
+        o = n2w.walk_options(walks_per_point=W, epsilon=5e-4, seed=1)
+        ms = None
+        for _ in range(2):
+            t.start()
+            call("n2w_wos_estimate", bvh.handle, C.byref(pb), dp.ptr, n, C.byref(o), st.struct(), None, ws.ptr, None)
+            t.stop()
+            ms = t.ms()
+        r = st.download()
+        var = float(np.mean(r["sample_variance"]))
+        mse = float(np.mean((r["mean"] - ex) ** 2))
+        return ms / 1e3 / (n * W), var, max(mse - var / W, 0.0)
+
+    # Both estimators are unbiased (up to the epsilon shell), so the time uses
+    # bias^2 = 0; the measured MSE - var/N is reported with its standard error
+    # (about sqrt(2/n) var/N), which on a subsample exceeds the target itself.
+    tp, vp, b2 = plain(problem)
+    se_b2 = float(np.sqrt(2.0 / n) * vp / W)
+    out["plain_wos"] = {"s_per_walk": tp, "var_per_walk": vp, "bias2_estimate": b2, "bias2_stderr": se_b2,
+                        "seconds": nc.time_to_mse(target, P * tp, vp, 0.0)}
+    pk = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
+    pk.source_samples = 16
+    tk, vk, bk = plain(pk)
+    out["plain_wos_16_source_samples"] = {"s_per_walk": tk, "var_per_walk": vk, "bias2_estimate": bk,
+                                          "seconds": nc.time_to_mse(target, P * tk, vk, 0.0)}
+    cache = n2w.Cache(n2w.cache_config())
+    t.start()
+    losses = nc.train(cache, bvh, problem, mesh, steps=train_steps, batch=65536, walks_per_label=32, epsilon=5e-4)
+    t.stop()
+    train_s = t.ms() / 1e3
+
+    def level(coarse, resid):
+        o = nc.nc2lmc_options(mesh, coarse_walks=coarse, residual_walks=resid, depth_m=8, epsilon=5e-4, seed=7)
+        ms, r = None, None
+        for _ in range(2):
+            t.start()
+            r = nc.nc2lmc(bvh, problem, cache, x, o, d_points=dp)
+            t.stop()
+            ms = t.ms()
+        return ms / 1e3 / (n * max(coarse, resid)), r
+
+    tc, rc = level(W, 0)
+    tr, rr = level(0, W)
+    vc = float(np.mean(rc["coarse"]["sample_variance"]))
+    vr = float(np.mean(rr["residual"]["sample_variance"]))
+    est = rc["coarse"]["mean"] + rr["residual"]["mean"]
+    mse = float(np.mean((est - ex) ** 2))
+    per16 = (vc + 16 * vr, tc + tr / 16)  # (variance, cost) per coarse walk with Nr = Nc/16
+    t16 = nc.time_to_mse(target, P * per16[1], per16[0], 0.0, train_s)
+    opt = (np.sqrt(vc * tc) + np.sqrt(vr * tr)) ** 2
+    out["nc2lmc"] = {"train_s": train_s, "train_steps": train_steps, "train_batch": 65536, "walks_per_label": 32,
+                     "loss_first_last": [float(losses[0]), float(losses[-1])], "depth_m": 8, "residual_fraction": 1 / 16,
+                     "s_per_coarse_walk": tc, "s_per_residual_walk": tr, "var_coarse": vc, "var_residual": vr,
+                     "mse_256c_256r": mse, "seconds": t16,
+                     "seconds_optimal_allocation": train_s + P * opt / target,
+                     "optimal_residual_fraction": float(np.sqrt((vr / tr) / (vc / tc)))}
+    out["speedup_nc2lmc_vs_plain"] = (out["plain_wos"]["seconds"] / t16) if t16 else None
+    out["method"] = ("per-walk cost by CUDA events and per-walk variance on a subsample; "
+                     "MSE(N) = bias^2 + var/N extrapolated to the full slice")
+    return out
 
 
 def run_reference(args):
@@ -204,6 +289,7 @@ def main():
     ap.add_argument("--impl", default="n2w", choices=["n2w", "reference"])
     ap.add_argument("--walks", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MSE comparison (NC+2LMC vs plain)")
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N slice points (smaller workload for profiler captures; "
                          "the default 0 runs the full slice)")
@@ -337,6 +423,9 @@ def main():
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                        "sample": f"failed: {e}"}
         wsteps_per_walk = c_last["steps"] / max(c_last["walks"], 1)
+        ttm = None
+        if not args.no_ttm and world == 1 and args.points == 0:
+            ttm = time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -356,8 +445,7 @@ def main():
             "clocks": clocks.summary(),
             "accuracy": {"mse_vs_fp64_exact": mse, "mean_estimator_variance": var_part, "bias2_estimate": bias2,
                          "walks_per_point": W, "mean_steps_per_walk": wsteps_per_walk},
-            "time_to_mse_1e-4_s_plain_wos_extrapolated": (kernel_ms / 1e3) * var_part / max(1e-4 - bias2, 1e-12)
-            if bias2 < 1e-4 else None,
+            "time_to_mse_1e-4": ttm,
             "counters_last_step": c_last,
             "walks_per_s": c_last["walks"] / (kernel_ms / 1e3),
         }

@@ -186,6 +186,8 @@ typedef struct n2w_problem {
   int32_t charge_count;     /* for N2W_BC_CHARGES_SEEDED */
   float omega;              /* for N2W_BC_POISSON_SINPROD */
   float charges[N2W_MAX_CHARGES][4]; /* x, y, z, amplitude */
+  int32_t source_samples;   /* N2W_SOURCE_BALL: points averaged per ball (0 or 1 = one, max 64) */
+  int32_t reserved;
 } n2w_problem;
 
 /* Seeded charge set: centres uniform in the spherical shell r in [r_min, r_max]
@@ -367,6 +369,59 @@ int n2w_cache_set_params(n2w_cache* cache, const float* h_fp32);
 /* Versioned binary checkpoint: config, step, parameters, Adam moments. */
 int n2w_cache_save(const n2w_cache* cache, const char* path);
 int n2w_cache_load(const char* path, n2w_cache** out);
+
+/* ---- neural-cache estimators -------------------------------------------- */
+/* n points uniform in the interior of the closed mesh: Philox candidates in
+ * [box_lo, box_hi] kept by +x ray parity (the reference samples its training
+ * set the same way on the CPU, src/tools/eval_tcnn_nc_wos.cu:437-491).
+ * Synchronises; *h_accepted_out (may be NULL) = points produced. */
+int n2w_sample_interior(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n,
+                        uint64_t seed, n2w_vec3* d_points_out, int64_t* h_accepted_out,
+                        n2w_stream_t stream);
+/* Unit-cube cache inputs: clamp((x - input_min) / input_extent, 0, 1)
+ * (reference nc_fill_inputs_kernel, src/cuda/cubql_bvh.cu:1359-1370). */
+int n2w_map_to_unit(const n2w_vec3* d_points, int64_t n, const float* input_min,
+                    const float* input_extent, float* d_inputs, n2w_stream_t stream);
+
+typedef struct n2w_nc_train_options {
+  int32_t steps;            /* training steps */
+  int32_t batch;            /* fresh interior points per step */
+  int32_t walks_per_label;  /* WoS walks averaged into each label */
+  int32_t max_steps;
+  float epsilon;
+  float step_scale;
+  uint64_t seed;
+  float input_min[3];
+  float input_extent[3];
+  float sample_lo[3];       /* box for interior sampling */
+  float sample_hi[3];
+} n2w_nc_train_options;
+/* Online training: per step, fresh interior points, WoS labels (mean of
+ * walks_per_label walks, per-point FP64 on the device), one Adam step on the L2
+ * loss.  h_losses (may be NULL) receives each step's batch loss (synchronises
+ * every step when given). */
+int n2w_nc_train(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* problem,
+                 const n2w_nc_train_options* options, float* h_losses, n2w_stream_t stream);
+
+typedef struct n2w_nc2lmc_options {
+  int32_t coarse_walks;     /* walks per point truncated at depth_m, closed by the cache */
+  int32_t residual_walks;   /* walks per point continued to the boundary (0 = NC-WoS only) */
+  int32_t depth_m;
+  int32_t max_steps;
+  float epsilon;
+  float step_scale;
+  uint64_t seed;
+  float input_min[3];
+  float input_extent[3];
+  int32_t point_batch;      /* points per internal batch (0 = auto) */
+} n2w_nc2lmc_options;
+/* NC+2LMC: coarse stats accumulate A_m + C(X_m) (or the full walk value when it
+ * stops before depth m); residual stats accumulate W(X_m) - C(X_m) (0 when it
+ * stopped before m).  Estimate = mean(coarse) + mean(residual); estimator
+ * variance = var_c / N_c + var_r / N_r. */
+int n2w_nc2lmc_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_cache* cache,
+                        const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* options,
+                        n2w_point_stats coarse, n2w_point_stats residual, n2w_stream_t stream);
 
 /* ---- thin device-memory helpers for callers without a CUDA binding ------ */
 int n2w_device_count(int* out);

@@ -554,10 +554,10 @@ __global__ void __launch_bounds__(kTrainBlock) train_kernel(const NetArgs a) {
 // clears the gradient.
 __global__ void adam_kernel(float* __restrict__ p, __half* __restrict__ ph, float* __restrict__ g,
                             float* __restrict__ m, float* __restrict__ v, int64_t n, float lr, float b1, float b2,
-                            float eps, float bc1, float bc2) {
+                            float eps, float bc1, float bc2, float gscale) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float gi = g[i];
+  const float gi = g[i] * gscale;
   const float mi = b1 * m[i] + (1.0f - b1) * gi;
   const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
   m[i] = mi;
@@ -567,6 +567,11 @@ __global__ void adam_kernel(float* __restrict__ p, __half* __restrict__ ph, floa
   p[i] = pn;
   ph[i] = __float2half_rn(pn);
   g[i] = 0.0f;
+}
+
+__global__ void scale_kernel(float* __restrict__ g, int64_t n, float s) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) g[i] *= s;
 }
 
 __global__ void to_half_kernel(const float* __restrict__ p, __half* __restrict__ ph, int64_t n) {
@@ -875,10 +880,17 @@ int n2w_cache_gradients(n2w_cache* c, const float* d_inputs, const float* d_targ
     a.targets = d_targets;
     a.outputs = d_outputs;
     a.n = n;
-    a.loss_scale = 2.0f / static_cast<float>(n);  // d/dy of mean (y - t)^2
+    // The backward runs on n * dL/dy = 2 (y - t): O(1) values keep FP16
+    // activations' gradients out of the subnormal range; the 1/n is applied to
+    // the FP32 gradient afterwards.
+    a.loss_scale = 2.0f;
     a.loss_sum = c->d_loss;
     N2W_CUDA(cudaMemsetAsync(c->d_loss, 0, sizeof(float), stream));
     launch_train(a, stream);
+    const int b = 256;
+    scale_kernel<<<static_cast<unsigned>((c->n_total + b - 1) / b), b, 0, stream>>>(c->d_g, c->n_total,
+                                                                                     1.0f / static_cast<float>(n));
+    N2W_CUDA(cudaGetLastError());
   });
 }
 
@@ -891,7 +903,7 @@ int n2w_cache_train_step(n2w_cache* c, const float* d_inputs, const float* d_tar
     a.inputs = d_inputs;
     a.targets = d_targets;
     a.n = n;
-    a.loss_scale = 2.0f / static_cast<float>(n);
+    a.loss_scale = 2.0f;  // n * dL/dy; the 1/n is applied inside the Adam update
     a.loss_sum = c->d_loss;
     N2W_CUDA(cudaMemsetAsync(c->d_loss, 0, sizeof(float), stream));
     launch_train(a, stream);
@@ -901,7 +913,8 @@ int n2w_cache_train_step(n2w_cache* c, const float* d_inputs, const float* d_tar
     const float bc2 = 1.0f - std::pow(b2, static_cast<float>(c->step));
     const int b = 256;
     adam_kernel<<<static_cast<unsigned>((c->n_total + b - 1) / b), b, 0, stream>>>(
-        c->d_p, c->d_ph, c->d_g, c->d_m, c->d_v, c->n_total, c->cfg.learning_rate, b1, b2, c->cfg.epsilon, bc1, bc2);
+        c->d_p, c->d_ph, c->d_g, c->d_m, c->d_v, c->n_total, c->cfg.learning_rate, b1, b2, c->cfg.epsilon, bc1, bc2,
+        1.0f / static_cast<float>(n));
     N2W_CUDA(cudaGetLastError());
     if (h_loss_out) {
       float l = 0.0f;

@@ -57,6 +57,42 @@ __device__ __forceinline__ float green_radius_fraction(float u) {
 
 __device__ __forceinline__ double shfl_xor_d(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
 
+// Dirichlet value at the terminal closest point.
+__device__ __forceinline__ float boundary_value(const WalkArgs& a, dev::V3 p) {
+  return problem_u<float>(a.problem, p.x, p.y, p.z);
+}
+
+// Source contribution of the ball B(x, R): (R^2/6) * f at the ball centre
+// (reference rule) or averaged over `source_samples` points drawn from the
+// ball's Green's function.  Sample 0 takes its radius fraction from word u2 of
+// the step's stream-0 draw and its direction from stream 1; samples k >= 1 use
+// stream 1 + k.
+__device__ __forceinline__ float ball_source(const WalkArgs& a, dev::V3 x, float R, uint64_t wid, int step,
+                                         uint32_t u2) {
+  float f;
+  if (a.source_center) {
+    f = problem_f<float>(a.problem, x.x, x.y, x.z);
+  } else {
+    const float tfrac = green_radius_fraction(u01(u2));
+    const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                   static_cast<uint32_t>(step), 1u},
+                                a.k0, a.k1);
+    const dev::V3 w = unit_sphere(r2.x, r2.y);
+    const float rho = R * tfrac;
+    f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
+    for (int k = 1; k < a.source_samples; ++k) {
+      const U4 rk = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
+                                     static_cast<uint32_t>(step), 1u + static_cast<uint32_t>(k)},
+                                  a.k0, a.k1);
+      const float rk_rho = R * green_radius_fraction(u01(rk.x));
+      const dev::V3 wk = unit_sphere(rk.y, rk.z);
+      f += problem_f<float>(a.problem, x.x + rk_rho * wk.x, x.y + rk_rho * wk.y, x.z + rk_rho * wk.z);
+    }
+    if (a.source_samples > 1) f *= 1.0f / static_cast<float>(a.source_samples);
+  }
+  return (R * R) * (1.0f / 6.0f) * f;
+}
+
 // Warp-collective flush of per-lane chunk accumulators into per-point FP64
 // totals: lanes are grouped by point id, each group is reduced by a shuffle
 // butterfly (non-members contribute zero) and its lowest lane issues the atomics.
@@ -191,7 +227,7 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
 //    so the walk updates run for many lanes at once and no lane waits for
 //    another lane's whole traversal.
 template <int kOut, int kWalk>
-__global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArgs a) {
+__global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_kernel(const __grid_constant__ WalkArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t t_start = (a.deadline_ns > 0) ? global_ns() : 0;
 
@@ -241,7 +277,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArg
       const bool forced = rel >= a.max_steps;
       const bool stop = d <= a.eps || forced || !isfinite(d) || hit.id == INT32_MAX;
       if (stop || (kWalk == N2W_WALK_PREFIX && step >= a.depth_m)) {
-        const float value = stop ? src + problem_u<float>(a.problem, hit.cp.x, hit.cp.y, hit.cp.z) : src;
+        const float value = stop ? src + boundary_value(a, hit.cp) : src;
         ++c_walks;
         c_steps += static_cast<uint32_t>(step);
         c_forced += forced ? 1u : 0u;
@@ -310,23 +346,19 @@ __global__ void __launch_bounds__(kWalkerMaxThreads) walker_kernel(const WalkArg
                                     static_cast<uint32_t>(step), 0u},
                                  a.k0, a.k1);
       const dev::V3 dir = unit_sphere(r.x, r.y);
-      if (a.has_source) {
-        float f;
-        if (a.source_center) {
-          f = problem_f<float>(a.problem, x.x, x.y, x.z);
-        } else {
-          const float tfrac = green_radius_fraction(u01(r.z));
-          const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
-                                         static_cast<uint32_t>(step), 1u},
-                                      a.k0, a.k1);
-          const dev::V3 w = unit_sphere(r2.x, r2.y);
-          const float rho = R * tfrac;
-          f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
-        }
-        src += (R * R) * (1.0f / 6.0f) * f;
-      }
+      if (a.has_source) src += ball_source(a, x, R, wid, step, r.z);
       const int prev_slot = hit.slot;
-      x = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
+      const dev::V3 xn = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
+      if (!(xn.x >= a.box_lo[0] && xn.x <= a.box_hi[0] && xn.y >= a.box_lo[1] && xn.y <= a.box_hi[1] &&
+            xn.z >= a.box_lo[2] && xn.z <= a.box_hi[2])) {
+        // A walk from an interior point stays inside the mesh; leaving the
+        // domain box means the start point was outside (a misclassified sample).
+        // Stop it as forced, scored at the current closest point, instead of
+        // letting it wander the unbounded exterior.
+        step = cont0 + a.max_steps;
+        continue;
+      }
+      x = xn;
       ++step;
       // Seed the next query with two real candidates (previous closest
       // triangle, seed-grid triangle at x); the exact answer is unchanged.
@@ -561,6 +593,7 @@ void validate_problem(const n2w_problem& p) {
   N2W_REQUIRE(ok, "unsupported boundary mode " + std::to_string(m));
   N2W_REQUIRE(p.source_sampling == N2W_SOURCE_BALL || p.source_sampling == N2W_SOURCE_CENTER,
               "source_sampling must be N2W_SOURCE_BALL or N2W_SOURCE_CENTER");
+  N2W_REQUIRE(p.source_samples >= 0 && p.source_samples <= 64, "source_samples must be in [0, 64]");
   if (m == N2W_BC_CHARGES_SEEDED) {
     N2W_REQUIRE(p.charge_count >= 1 && p.charge_count <= N2W_MAX_CHARGES, "charge_count must be in [1, 16]");
   }
@@ -572,6 +605,10 @@ WalkArgs make_walk_args(const n2w_bvh& bvh, const n2w_problem& problem, const n2
   a.nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
   a.tris = reinterpret_cast<const float4*>(bvh.d_tris);
   a.grid = seed_grid_of(bvh);
+  for (int k = 0; k < 3; ++k) {
+    a.box_lo[k] = bvh.d_seed ? bvh.seed_lo[k] : -1.0e30f;
+    a.box_hi[k] = bvh.d_seed ? bvh.seed_lo[k] + bvh.seed_h * static_cast<float>(bvh.seed_n) : 1.0e30f;
+  }
   a.points = d_points;
   a.walks_per_point = o.walks_per_point;
   a.chunk = o.chunk > 0 ? std::min(o.chunk, o.walks_per_point) : std::min(kDefaultChunk, o.walks_per_point);
@@ -586,6 +623,7 @@ WalkArgs make_walk_args(const n2w_bvh& bvh, const n2w_problem& problem, const n2
   a.problem = problem;
   a.has_source = problem_has_source(problem) ? 1 : 0;
   a.source_center = problem.source_sampling == N2W_SOURCE_CENTER ? 1 : 0;
+  a.source_samples = problem.source_samples > 1 ? problem.source_samples : 1;
   a.deadline_ns = o.deadline_ns;
   return a;
 }

@@ -13,6 +13,9 @@ constexpr int kOutSamples = 1;  // per-sample value / steps / flags (reference l
 constexpr int kOutPrefix = 2;   // per-sample prefix records for the cache levels
 
 constexpr int kWalkerMaxThreads = 256;
+// Resident 256-thread blocks the register budget must allow (64 registers per
+// thread): the traversal hides L1/L2 latency with warps, so occupancy matters.
+constexpr int kWalkerMinBlocks = 4;
 constexpr int kDefaultWalkerThreads = 128;
 constexpr int kDefaultChunk = 8;
 constexpr int kDefaultRegen = 12;
@@ -21,6 +24,7 @@ struct WalkArgs {
   const float4* nodes;
   const float4* tris;
   dev::SeedGrid grid;
+  float box_lo[3], box_hi[3];  // domain box: the mesh box grown by 20 % (walks never leave it)
   const n2w_vec3* points;
   // Per-point first query (closest point + d2, id + slot): every walk of a
   // point starts with the same query, computed once by a pre-pass.
@@ -38,6 +42,7 @@ struct WalkArgs {
   uint32_t k0, k1;
   int has_source;
   int source_center;
+  int source_samples;  // points averaged per ball (>= 1)
   int64_t deadline_ns;
   n2w_problem problem;
   // kOutStats

@@ -54,7 +54,8 @@ class BvhStats(C.Structure):
 
 class Problem(C.Structure):
     _fields_ = [("mode", C.c_int32), ("source_sampling", C.c_int32), ("charge_count", C.c_int32),
-                ("omega", C.c_float), ("charges", (C.c_float * 4) * N2W_MAX_CHARGES)]
+                ("omega", C.c_float), ("charges", (C.c_float * 4) * N2W_MAX_CHARGES), ("source_samples", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class WalkOptions(C.Structure):
@@ -80,6 +81,19 @@ class CacheConfig(C.Structure):
                 ("base_resolution", C.c_float), ("per_level_scale", C.c_float), ("max_resolution", C.c_float),
                 ("n_neurons", C.c_int32), ("n_hidden_layers", C.c_int32), ("learning_rate", C.c_float),
                 ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float), ("seed", C.c_uint64)]
+
+
+class NcTrainOptions(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("walks_per_label", C.c_int32),
+                ("max_steps", C.c_int32), ("epsilon", C.c_float), ("step_scale", C.c_float), ("seed", C.c_uint64),
+                ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3), ("sample_lo", C.c_float * 3),
+                ("sample_hi", C.c_float * 3)]
+
+
+class Nc2lmcOptions(C.Structure):
+    _fields_ = [("coarse_walks", C.c_int32), ("residual_walks", C.c_int32), ("depth_m", C.c_int32),
+                ("max_steps", C.c_int32), ("epsilon", C.c_float), ("step_scale", C.c_float), ("seed", C.c_uint64),
+                ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3), ("point_batch", C.c_int32)]
 
 
 P = C.c_void_p
@@ -147,6 +161,11 @@ _SIGS = {
     "n2w_cache_set_params": (I, [P, P]),
     "n2w_cache_save": (I, [P, C.c_char_p]),
     "n2w_cache_load": (I, [C.c_char_p, PP]),
+    "n2w_sample_interior": (I, [P, P, P, I64, C.c_uint64, P, C.POINTER(I64), P]),
+    "n2w_map_to_unit": (I, [P, I64, P, P, P, P]),
+    "n2w_nc_train": (I, [P, P, C.POINTER(Problem), C.POINTER(NcTrainOptions), P, P]),
+    "n2w_nc2lmc_estimate": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,
+                                PointStats, P]),
     "n2w_device_count": (I, [C.POINTER(I)]),
     "n2w_set_device": (I, [I]),
     "n2w_malloc": (I, [PP, C.c_size_t]),

@@ -218,6 +218,8 @@ struct Problem {
   int32_t charge_count;
   float omega;
   float charges[16][4];
+  int32_t source_samples;
+  int32_t reserved;
 };
 
 float safe_sqrt(float r2) { return std::sqrt(std::fmax(r2, 1.0e-12f)); }
@@ -436,6 +438,20 @@ void oracle_wos(const void* nodes, const void* tris, const void* problem, const 
             const float rr2 = std::sqrt(std::fmax(0.0f, 1.0f - z2 * z2));
             const float rho = R * t;
             f = f_value(pb, {x.x + rho * rr2 * std::cos(phi2), x.y + rho * rr2 * std::sin(phi2), x.z + rho * z2});
+            const int K = pb.source_samples > 1 ? pb.source_samples : 1;
+            for (int k = 1; k < K; ++k) {
+              // extra in-ball samples: Philox stream 1 + k (radius, direction)
+              const U4 rk = philox(U4{static_cast<uint32_t>(w), static_cast<uint32_t>(w >> 32),
+                                      static_cast<uint32_t>(step), 1u + static_cast<uint32_t>(k)},
+                                   k0, k1);
+              const float ak = std::acos(std::fmin(1.0f, std::fmax(-1.0f, 1.0f - 2.0f * u01(rk.x))));
+              const float rhok = R * (0.5f + std::cos((ak - 6.283185307179586f) / 3.0f));
+              const float zk = 1.0f - 2.0f * u01(rk.y);
+              const float phk = 2.0f * 3.14159265358979323846f * u01(rk.z);
+              const float rrk = std::sqrt(std::fmax(0.0f, 1.0f - zk * zk));
+              f += f_value(pb, {x.x + rhok * rrk * std::cos(phk), x.y + rhok * rrk * std::sin(phk), x.z + rhok * zk});
+            }
+            if (K > 1) f *= 1.0f / static_cast<float>(K);
           }
           src += R * R * (1.0f / 6.0f) * f;
         }

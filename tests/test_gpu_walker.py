@@ -103,6 +103,28 @@ def test_poisson_ball_sampling_unbiased_center_rule_biased(gpu):
     assert np.sqrt(np.mean(err_c ** 2)) > 3 * np.sqrt(np.mean(err_b ** 2))
 
 
+def test_poisson_multi_sample_source_parity_and_variance(gpu, small_scene):
+    """K in-ball source samples per ball: GPU vs oracle over 8 seeds (3 sigma), and
+    the per-walk variance drops relative to one sample per ball."""
+    m, bvh, nodes, tris, pts = small_scene
+    W = 512
+    p1 = gpu.problem_sinprod(3 * np.pi, gpu.N2W_SOURCE_BALL)
+    p4 = gpu.problem_sinprod(3 * np.pi, gpu.N2W_SOURCE_BALL)
+    p4.source_samples = 4
+    gm, gv, om, ov = [], [], [], []
+    for seed in range(1, 9):
+        r, _ = run(gpu, bvh, p4, pts, walks_per_point=W, epsilon=1e-3, seed=seed)
+        o = oracle.wos(nodes, tris, bytes(p4), pts, W, 256, 1e-3, 0.999, *key_words(seed))
+        gm.append(r["mean"]); gv.append(r["stderr"] ** 2)
+        om.append(o["mean"]); ov.append(o["stderr"] ** 2)
+    gm, gv, om, ov = map(np.array, (gm, gv, om, ov))
+    sigma = np.sqrt(gv.mean(0) / 8 + ov.mean(0) / 8)
+    assert np.all(np.abs(gm.mean(0) - om.mean(0)) <= 3 * sigma)
+    r1, _ = run(gpu, bvh, p1, pts, walks_per_point=8192, epsilon=1e-3, seed=11)
+    r4, _ = run(gpu, bvh, p4, pts, walks_per_point=8192, epsilon=1e-3, seed=11)
+    assert r4["sample_variance"].mean() < 0.6 * r1["sample_variance"].mean()
+
+
 def test_reference_poisson_modes_both_rules_unbiased(gpu, small_scene):
     """Harmonic sources (reference modes 30/31): the centre rule is exact and the
     ball sample agrees with it."""
@@ -187,6 +209,18 @@ def test_deadline_stops_walkers(gpu, small_scene):
     assert cnt["walks"] < 4096 * len(big)
     assert cnt["timed_out"] > 0
     assert r["count"].sum() == cnt["walks"]
+
+
+def test_walks_from_outside_points_stay_bounded(gpu, small_scene):
+    """A start point outside the closed mesh (e.g. a misclassified sample) must not
+    send walks into the unbounded exterior: they stop at the domain box as forced,
+    with finite values, in bounded time."""
+    m, bvh, nodes, tris, pts = small_scene
+    p = gpu.problem_sinprod(3 * np.pi, gpu.N2W_SOURCE_BALL)
+    outside = np.array([[1.3, 0.0, 0.0], [0.0, -1.25, 0.3], [0.9, 0.9, 0.9]], np.float32)
+    r, cnt = run(gpu, bvh, p, outside, walks_per_point=4096, epsilon=1e-3)
+    assert np.all(np.isfinite(r["mean"])) and np.all(np.isfinite(r["sample_variance"]))
+    assert cnt["walks"] == 3 * 4096 and cnt["forced"] > 0
 
 
 def test_invalid_options(gpu, small_scene):
