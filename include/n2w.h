@@ -80,6 +80,15 @@ int n2w_mesh_copy_out(const n2w_mesh* mesh, float* vertices, uint32_t* triangles
 int n2w_mesh_bounds(const n2w_mesh* mesh, float* bounds_out);
 /* Number of triangles with |cross(b-a,c-a)|^2 <= area2_epsilon (reference closest_point.cpp:70-83). */
 int n2w_mesh_count_degenerate(const n2w_mesh* mesh, float area2_epsilon, int64_t* out);
+/* Host brute-force closest point over every triangle (reference
+ * closest_point_bruteforce, src/geometry/closest_point.cpp:50-68): squared
+ * distance, closest point (xyz) and triangle id (lowest id on exact ties) for n
+ * host points, with the device kernel's arithmetic.  threads <= 0 uses all
+ * hardware threads.  Any output may be NULL.  Used by the probes to validate. */
+int n2w_mesh_closest_point_host(const n2w_mesh* mesh, const float* xyz, int64_t n, float* d2_out,
+                                float* closest_out, int* tri_out, int threads);
+/* Mesh name ("procedural_bumpy_sphere", file stem of a loaded mesh, ...); owned by the mesh. */
+const char* n2w_mesh_name(const n2w_mesh* mesh);
 void n2w_mesh_free(n2w_mesh* mesh);
 
 /* ---- BVH + closest point ----------------------------------------------- */
@@ -145,6 +154,16 @@ int n2w_bvh_inside_device(const n2w_bvh* bvh, const n2w_vec3* d_points, int quer
  * frame_out[4] = u_min, u_max, v_min, v_max (may be NULL). */
 int n2w_slice_points(const float* bounds6, const char* view, float plane, int width, int height,
                      float padding_fraction, int preserve_aspect, float* points_out, float* frame_out);
+/* Same grid with every choice explicit: frame_in[4] (u_min, u_max, v_min, v_max)
+ * replaces the padded bounds when not NULL (bounds6 may then be NULL); rule picks
+ * the pixel-coordinate rounding: N2W_SLICE_RULE_RENDER u_min + du * (i / (n-1))
+ * (reference renderer, cubql_bvh.cu:1013-1017) or N2W_SLICE_RULE_EVAL
+ * u_min + (du * i) / (n-1) (reference NC evaluator, eval_tcnn_nc_wos.cu:393). */
+#define N2W_SLICE_RULE_RENDER 0
+#define N2W_SLICE_RULE_EVAL 1
+int n2w_slice_points_ex(const float* bounds6, const float* frame_in, const char* view, float plane, int width,
+                        int height, float padding_fraction, int preserve_aspect, int rule, float* points_out,
+                        float* frame_out);
 /* Seed grid built with the BVH: (n+1)^3 lattice nodes lo + h*(i,j,k); slot of
  * the triangle nearest each node (leaf order).  Queries test that triangle first,
  * so their traversal starts with a tight bound.  Any output may be NULL. */
@@ -378,6 +397,11 @@ int n2w_cache_load(const char* path, n2w_cache** out);
 int n2w_sample_interior(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n,
                         uint64_t seed, n2w_vec3* d_points_out, int64_t* h_accepted_out,
                         n2w_stream_t stream);
+/* Same, also reporting the candidates drawn (*h_candidates_out, may be NULL);
+ * accepted / candidates estimates the interior volume fraction of the box. */
+int n2w_sample_interior_ex(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n,
+                           uint64_t seed, n2w_vec3* d_points_out, int64_t* h_accepted_out,
+                           int64_t* h_candidates_out, n2w_stream_t stream);
 /* Unit-cube cache inputs: clamp((x - input_min) / input_extent, 0, 1)
  * (reference nc_fill_inputs_kernel, src/cuda/cubql_bvh.cu:1359-1370). */
 int n2w_map_to_unit(const n2w_vec3* d_points, int64_t n, const float* input_min,
@@ -422,6 +446,75 @@ typedef struct n2w_nc2lmc_options {
 int n2w_nc2lmc_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_cache* cache,
                         const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* options,
                         n2w_point_stats coarse, n2w_point_stats residual, n2w_stream_t stream);
+
+/* Sample counts of an NC+2LMC run (device struct; the call ADDS to it, the
+ * caller zeroes it).  Mirrors the NC evaluator's host-side counting
+ * (src/tools/eval_tcnn_nc_wos.cu:527-533, 548-549). */
+typedef struct n2w_nc2lmc_counters {
+  unsigned long long coarse_cache_queries;   /* coarse walks closed by the cache */
+  unsigned long long coarse_forced;          /* coarse walks stopped by max_steps */
+  unsigned long long coarse_overflow;        /* coarse walks with a traversal overflow */
+  unsigned long long residual_cache_queries; /* residual walks that reached depth m */
+  unsigned long long residual_forced;
+  unsigned long long residual_overflow;
+} n2w_nc2lmc_counters;
+/* n2w_nc2lmc_estimate plus counters (d_counters may be NULL).  cache == NULL
+ * selects the analytic cache C(x) = u(x), the exact solution of the problem:
+ * the reference's debug-only oracle levels (src/cuda/wos_wavefront.cu:140-149,
+ * methods oracle_coarse / oracle_residual / oracle_2lmc). */
+int n2w_nc2lmc_estimate_ex(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_cache* cache,
+                           const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* options,
+                           n2w_point_stats coarse, n2w_point_stats residual, n2w_nc2lmc_counters* d_counters,
+                           n2w_stream_t stream);
+
+/* Training labels over a fixed point set, mirroring launch_nc_update_labels
+ * (include/n2wos/tcnn_nc_wos.hpp:79-86, kernel src/cuda/cubql_bvh.cu:1372-1420).
+ * Each call is one refresh: N2W_LABEL_WOS runs walks_per_point more walks per
+ * point into the caller-owned running accumulators `accum` (zero them before
+ * refresh 0) and writes targets = running mean of every walk so far;
+ * N2W_LABEL_EXACT writes the exact solution.  Inputs are the points mapped to
+ * the unit cube.  d_workspace: n2w_wos_workspace_bytes(n) bytes or NULL. */
+#define N2W_LABEL_EXACT 0 /* reference NcLabelSource::ExactAnalytic */
+#define N2W_LABEL_WOS 1   /* reference NcLabelSource::WosSupervision */
+typedef struct n2w_nc_label_options {
+  int32_t walks_per_point;
+  int32_t max_steps;
+  float epsilon;
+  float step_scale;
+  uint64_t seed;
+  int32_t refresh_index;
+  int32_t label_source;
+  float input_min[3];
+  float input_extent[3];
+  int32_t block_size;       /* walker block size (0 = tuned default) */
+  int32_t reserved;
+} n2w_nc_label_options;
+int n2w_nc_update_labels(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
+                         const n2w_nc_label_options* options, n2w_point_stats accum, float* d_inputs,
+                         float* d_targets, void* d_workspace, n2w_stream_t stream);
+
+/* ---- device utilities ---------------------------------------------------- */
+/* u(x) of the problem at n device points, evaluated in FP64 and stored as FP32. */
+int n2w_problem_exact_device(const n2w_problem* problem, const n2w_vec3* d_points, int64_t n, float* d_u_out,
+                             n2w_stream_t stream);
+/* Analytic cache: outputs = u(input_min + inputs * input_extent) for unit-cube
+ * inputs (float[3n]), the stand-in for C(x) in the oracle levels. */
+int n2w_oracle_cache_infer(const n2w_problem* problem, const float* d_inputs, int64_t n, const float* input_min,
+                           const float* input_extent, float* d_outputs, n2w_stream_t stream);
+/* n unit-cube samples from Philox(seed; sample, step) and, when d_targets is
+ * not NULL, targets u(input_min + x * input_extent).  The cache probe's batch
+ * generator (src/tools/probe_tcnn_cache.cu:233-250) with a counter-based RNG. */
+int n2w_fill_unit_samples(const n2w_problem* problem, int64_t n, uint64_t seed, uint32_t step,
+                          const float* input_min, const float* input_extent, float* d_inputs, float* d_targets,
+                          n2w_stream_t stream);
+/* d_acc4[0..3] += sum pred, sum exact, sum (pred-exact)^2, sum |pred-exact|
+ * (FP64): the cache probe's downstream consumer (probe_tcnn_cache.cu:251-262). */
+int n2w_compare_accumulate(const float* d_pred, const float* d_exact, int64_t n, double* d_acc4,
+                           n2w_stream_t stream);
+/* d_counts3[0..2] += number of nonzero entries of needs_cache (u8), forced and
+ * overflow (int32); any input may be NULL. */
+int n2w_count_samples(const uint8_t* d_needs_cache, const int* d_forced, const int* d_overflow, int64_t n,
+                      unsigned long long* d_counts3, n2w_stream_t stream);
 
 /* ---- thin device-memory helpers for callers without a CUDA binding ------ */
 int n2w_device_count(int* out);

@@ -33,12 +33,15 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{CUDA_HOME / 'include'}"]
 
-LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu"]
+LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu", "util.cu"]
 LIB_CPP = ["mesh.cpp", "bvh_build.cpp", "capi.cpp"]
 EXECUTABLES = {
     "n2wos_probe_cuda_bvh": ["probe_cuda_bvh.cpp"],
     "n2wos_probe_geometry_backends": ["probe_geometry_backends.cpp"],
     "n2wos_eval_wavefront_wos": ["eval_wavefront_wos.cpp"],
+    "n2wos_eval_tcnn_nc_wos": ["eval_tcnn_nc_wos.cpp"],
+    "n2wos_probe_tcnn_cache": ["probe_tcnn_cache.cpp"],
+    "n2wos_render_harmonic_slice": ["render_harmonic_slice.cpp"],
 }
 
 

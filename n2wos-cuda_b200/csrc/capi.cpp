@@ -183,8 +183,15 @@ const char* n2w_problem_mode_name(int mode) {
 
 int n2w_slice_points(const float* b, const char* view, float plane, int width, int height, float padding,
                      int preserve_aspect, float* points_out, float* frame_out) {
+  return n2w_slice_points_ex(b, nullptr, view, plane, width, height, padding, preserve_aspect, N2W_SLICE_RULE_RENDER,
+                             points_out, frame_out);
+}
+
+int n2w_slice_points_ex(const float* b, const float* frame_in, const char* view, float plane, int width, int height,
+                        float padding, int preserve_aspect, int rule, float* points_out, float* frame_out) {
   return guarded([&] {
-    N2W_REQUIRE(b && view, "null argument");
+    N2W_REQUIRE(view && (b || frame_in), "null argument");
+    N2W_REQUIRE(rule == N2W_SLICE_RULE_RENDER || rule == N2W_SLICE_RULE_EVAL, "bad pixel coordinate rule");
     N2W_REQUIRE(width > 0 && height > 0, "slice width/height must be positive");
     const std::string v(view);
     int ua, va, fa;
@@ -194,9 +201,19 @@ int n2w_slice_points(const float* b, const char* view, float plane, int width, i
     else throw Error(N2W_EINVAL, "slice view must be one of: xy, xz, yz");
     // Frame from the bounds, padded, then widened to the image aspect
     // (reference cubql_bvh.cu:90-112, 974-995), in the same float operations.
-    const float du0 = b[3 + ua] - b[ua], dv0 = b[3 + va] - b[va];
-    float u_min = b[ua] - padding * du0, u_max = b[3 + ua] + padding * du0;
-    float v_min = b[va] - padding * dv0, v_max = b[3 + va] + padding * dv0;
+    float u_min, u_max, v_min, v_max;
+    if (frame_in) {
+      u_min = frame_in[0];
+      u_max = frame_in[1];
+      v_min = frame_in[2];
+      v_max = frame_in[3];
+    } else {
+      const float du0 = b[3 + ua] - b[ua], dv0 = b[3 + va] - b[va];
+      u_min = b[ua] - padding * du0;
+      u_max = b[3 + ua] + padding * du0;
+      v_min = b[va] - padding * dv0;
+      v_max = b[3 + va] + padding * dv0;
+    }
     if (preserve_aspect) {
       const float du = u_max - u_min, dv = v_max - v_min;
       if (du > 0.0f && dv > 0.0f) {
@@ -222,11 +239,16 @@ int n2w_slice_points(const float* b, const char* view, float plane, int width, i
     }
     if (!points_out) return;
     for (int iy = 0; iy < height; ++iy) {
+      // The reference renderer scales by (i / (n-1)); its NC evaluator by (d * i) / (n-1).
+      const float fy = static_cast<float>(iy), ny = static_cast<float>(height - 1);
       const float pv = height == 1 ? 0.5f * (v_min + v_max)
-                                   : v_min + (v_max - v_min) * (static_cast<float>(iy) / static_cast<float>(height - 1));
+                       : rule == N2W_SLICE_RULE_RENDER ? v_min + (v_max - v_min) * (fy / ny)
+                                                       : v_min + (v_max - v_min) * fy / ny;
       for (int ix = 0; ix < width; ++ix) {
+        const float fx = static_cast<float>(ix), nx = static_cast<float>(width - 1);
         const float pu = width == 1 ? 0.5f * (u_min + u_max)
-                                    : u_min + (u_max - u_min) * (static_cast<float>(ix) / static_cast<float>(width - 1));
+                         : rule == N2W_SLICE_RULE_RENDER ? u_min + (u_max - u_min) * (fx / nx)
+                                                         : u_min + (u_max - u_min) * fx / nx;
         float* p = points_out + 3 * (static_cast<int64_t>(iy) * width + ix);
         p[ua] = pu;
         p[va] = pv;

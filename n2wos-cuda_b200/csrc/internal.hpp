@@ -99,4 +99,11 @@ void launch_inside(const n2w_bvh& bvh, const n2w_vec3* d_points, int n, uint8_t*
 
 int sm_count_current();
 
+// ---- device utilities (util.cu) ----
+void launch_oracle_cache(const n2w_problem& pb, const float* d_inputs, int64_t n, const float* in_min,
+                         const float* in_ext, float* d_out, cudaStream_t s);
+void launch_count_samples(const uint8_t* needs, const int* forced, const int* overflow, int64_t n,
+                          unsigned long long* d_counts, cudaStream_t s);
+void launch_exact(const n2w_problem& pb, const n2w_vec3* d_points, int64_t n, float* d_out, cudaStream_t s);
+
 }  // namespace n2w

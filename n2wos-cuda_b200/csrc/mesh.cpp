@@ -14,6 +14,7 @@
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <thread>
 #include <utility>
 
 #include "internal.hpp"
@@ -33,6 +34,73 @@ void require_valid(const n2w_mesh& m) {
       throw Error(N2W_EINVAL, "mesh triangle contains out-of-range vertex index");
     }
   }
+}
+
+// Closest point on triangle abc to p (Ericson, Real-Time Collision Detection
+// 5.1.5) with the device kernel's operation order, one IEEE operation per
+// step (this file is compiled without FP contraction), so host and device
+// agree bit for bit.
+struct HostHit {
+  float d2;
+  int id;
+  float cp[3];
+};
+
+inline float hdot(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+void closest_on_triangle(const float* p, const float* a, const float* b, const float* c, float* r) {
+  const float ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  const float ac[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+  const float ap[3] = {p[0] - a[0], p[1] - a[1], p[2] - a[2]};
+  const float d1 = hdot(ab, ap), d2 = hdot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) { std::memcpy(r, a, 12); return; }
+  const float bp[3] = {p[0] - b[0], p[1] - b[1], p[2] - b[2]};
+  const float d3 = hdot(ab, bp), d4 = hdot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) { std::memcpy(r, b, 12); return; }
+  const float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+    const float v = d1 / (d1 - d3);
+    for (int k = 0; k < 3; ++k) r[k] = a[k] + ab[k] * v;
+    return;
+  }
+  const float cq[3] = {p[0] - c[0], p[1] - c[1], p[2] - c[2]};
+  const float d5 = hdot(ab, cq), d6 = hdot(ac, cq);
+  if (d6 >= 0.0f && d5 <= d6) { std::memcpy(r, c, 12); return; }
+  const float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+    const float w = d2 / (d2 - d6);
+    for (int k = 0; k < 3; ++k) r[k] = a[k] + ac[k] * w;
+    return;
+  }
+  const float va = d3 * d6 - d5 * d4;
+  const float d43 = d4 - d3, d56 = d5 - d6;
+  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) {
+    const float w = d43 / (d43 + d56);
+    for (int k = 0; k < 3; ++k) r[k] = b[k] + (c[k] - b[k]) * w;
+    return;
+  }
+  const float q = 1.0f / ((va + vb) + vc);
+  const float v = vb * q, w = vc * q;
+  for (int k = 0; k < 3; ++k) r[k] = (a[k] + ab[k] * v) + ac[k] * w;
+}
+
+// Every triangle in id order; strict '<' keeps the lowest id on exact ties.
+HostHit closest_bruteforce(const n2w_mesh& m, float x, float y, float z) {
+  const float p[3] = {x, y, z};
+  HostHit best{INFINITY, -1, {x, y, z}};
+  for (size_t t = 0; t < m.triangles.size(); ++t) {
+    const auto& tri = m.triangles[t];
+    float r[3];
+    closest_on_triangle(p, m.vertices[tri[0]].data(), m.vertices[tri[1]].data(), m.vertices[tri[2]].data(), r);
+    const float dv[3] = {r[0] - p[0], r[1] - p[1], r[2] - p[2]};
+    const float dd = hdot(dv, dv);
+    if (dd < best.d2) {
+      best.d2 = dd;
+      best.id = static_cast<int>(t);
+      std::memcpy(best.cp, r, 12);
+    }
+  }
+  return best;
 }
 
 // Radius function of the reference generator (procedural_bumpy_sphere.cpp:12-17),
@@ -545,6 +613,43 @@ int n2w_mesh_count_degenerate(const n2w_mesh* mesh, float eps, int64_t* out) {
     *out = count;
   });
 }
+
+int n2w_mesh_closest_point_host(const n2w_mesh* mesh, const float* xyz, int64_t n, float* d2_out,
+                                float* closest_out, int* tri_out, int threads) {
+  return guarded([&] {
+    N2W_REQUIRE(mesh && (n == 0 || xyz), "null argument");
+    N2W_REQUIRE(n >= 0, "n must be non-negative");
+    require_valid(*mesh);
+    if (n == 0) return;
+    int nt = threads > 0 ? threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    nt = static_cast<int>(std::min<int64_t>(nt, std::max<int64_t>(1, n / 16)));
+    auto work = [&](int64_t lo, int64_t hi) {
+      for (int64_t i = lo; i < hi; ++i) {
+        const HostHit h = closest_bruteforce(*mesh, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        if (d2_out) d2_out[i] = h.d2;
+        if (closest_out) {
+          closest_out[3 * i + 0] = h.cp[0];
+          closest_out[3 * i + 1] = h.cp[1];
+          closest_out[3 * i + 2] = h.cp[2];
+        }
+        if (tri_out) tri_out[i] = h.id;
+      }
+    };
+    if (nt == 1) {
+      work(0, n);
+      return;
+    }
+    std::vector<std::thread> pool;
+    const int64_t per = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+      const int64_t lo = t * per, hi = std::min<int64_t>(n, lo + per);
+      if (lo < hi) pool.emplace_back(work, lo, hi);
+    }
+    for (auto& th : pool) th.join();
+  });
+}
+
+const char* n2w_mesh_name(const n2w_mesh* mesh) { return mesh ? mesh->name.c_str() : ""; }
 
 void n2w_mesh_free(n2w_mesh* mesh) { delete mesh; }
 

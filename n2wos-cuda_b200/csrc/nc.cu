@@ -101,6 +101,12 @@ extern "C" {
 
 int n2w_sample_interior(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n, uint64_t seed,
                         n2w_vec3* d_points_out, int64_t* h_accepted_out, n2w_stream_t stream) {
+  return n2w_sample_interior_ex(bvh, box_lo, box_hi, n, seed, d_points_out, h_accepted_out, nullptr, stream);
+}
+
+int n2w_sample_interior_ex(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n, uint64_t seed,
+                           n2w_vec3* d_points_out, int64_t* h_accepted_out, int64_t* h_candidates_out,
+                           n2w_stream_t stream) {
   return guarded([&] {
     N2W_REQUIRE(bvh && bvh->d_nodes && box_lo && box_hi, "null argument");
     N2W_REQUIRE(n >= 0, "n must be non-negative");
@@ -115,6 +121,7 @@ int n2w_sample_interior(const n2w_bvh* bvh, const float* box_lo, const float* bo
     N2W_CUDA(cudaStreamSynchronize(stream));
     const int64_t acc = static_cast<int64_t>(std::min<unsigned long long>(c[1], static_cast<unsigned long long>(n)));
     if (h_accepted_out) *h_accepted_out = acc;
+    if (h_candidates_out) *h_candidates_out = static_cast<int64_t>(std::min<unsigned long long>(c[0], 1000ull * n + 1000000ull));
     if (acc < n) throw Error(N2W_EINTERNAL, "interior sampling gave up: the box holds too little interior");
   });
 }
@@ -183,11 +190,60 @@ int n2w_nc_train(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* proble
   });
 }
 
+int n2w_nc_update_labels(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
+                         const n2w_nc_label_options* o, n2w_point_stats accum, float* d_inputs, float* d_targets,
+                         void* d_workspace, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(bvh && problem && o, "n2w_nc_update_labels: null argument");
+    N2W_REQUIRE(n >= 0, "n must be non-negative");
+    N2W_REQUIRE(o->label_source == N2W_LABEL_EXACT || o->label_source == N2W_LABEL_WOS, "bad label_source");
+    if (n == 0) return;
+    N2W_REQUIRE(d_points && d_inputs && d_targets, "n2w_nc_update_labels: null device pointer");
+    const float3 in_min = make_float3(o->input_min[0], o->input_min[1], o->input_min[2]);
+    const float3 in_ext = make_float3(o->input_extent[0], o->input_extent[1], o->input_extent[2]);
+    const int b = 256;
+    const unsigned grid = static_cast<unsigned>((n + b - 1) / b);
+    if (o->label_source == N2W_LABEL_EXACT) {
+      map_to_unit_kernel<<<grid, b, 0, stream>>>(d_points, n, in_min, in_ext, d_inputs);
+      N2W_CUDA(cudaGetLastError());
+      launch_exact(*problem, d_points, n, d_targets, stream);
+      return;
+    }
+    N2W_REQUIRE(o->walks_per_point > 0, "walks_per_point must be positive");
+    N2W_REQUIRE(accum.d_sum && accum.d_sum_sq && accum.d_count && accum.d_steps && accum.d_forced,
+                "WoS labels need the running accumulators");
+    n2w_walk_options wo{};
+    wo.walks_per_point = o->walks_per_point;
+    wo.max_steps = o->max_steps;
+    wo.epsilon = o->epsilon;
+    wo.step_scale = o->step_scale;
+    wo.seed = o->seed + 0x9E3779B97F4A7C15ull * static_cast<uint64_t>(o->refresh_index + 1);
+    wo.block_size = o->block_size;
+    wo.accumulate = 1;
+    const int st = n2w_wos_estimate(bvh, problem, d_points, n, &wo, accum, nullptr, d_workspace, stream);
+    if (st != N2W_OK) throw Error(st, n2w_last_error());
+    labels_kernel<<<grid, b, 0, stream>>>(d_points, accum.d_sum, accum.d_count, n, in_min, in_ext, d_inputs,
+                                          d_targets);
+    N2W_CUDA(cudaGetLastError());
+  });
+}
+
 int n2w_nc2lmc_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_cache* cache,
                         const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* o,
                         n2w_point_stats coarse, n2w_point_stats residual, n2w_stream_t stream) {
+  if (!cache) {
+    set_last_error("n2w_nc2lmc_estimate: null cache (n2w_nc2lmc_estimate_ex takes NULL for the analytic cache)");
+    return N2W_EINVAL;
+  }
+  return n2w_nc2lmc_estimate_ex(bvh, problem, cache, d_points, n, o, coarse, residual, nullptr, stream);
+}
+
+int n2w_nc2lmc_estimate_ex(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_cache* cache,
+                           const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* o,
+                           n2w_point_stats coarse, n2w_point_stats residual, n2w_nc2lmc_counters* d_counters,
+                           n2w_stream_t stream) {
   return guarded([&] {
-    N2W_REQUIRE(bvh && problem && cache && o, "null argument");
+    N2W_REQUIRE(bvh && problem && o, "null argument");
     N2W_REQUIRE(n >= 0, "n must be non-negative");
     N2W_REQUIRE(o->coarse_walks >= 0 && o->residual_walks >= 0 && o->depth_m >= 0 &&
                     (o->coarse_walks > 0 || o->residual_walks > 0),
@@ -234,7 +290,17 @@ int n2w_nc2lmc_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2
       status = n2w_wos_prefix_samples(bvh, problem, d_points + p0, np, &wo, mode, o->input_min, o->input_extent,
                                       inp, bnd, mode == N2W_WALK_RESIDUAL ? cont : nullptr, needs, stp, frc, ovf,
                                       stream);
-      if (status == N2W_OK) status = n2w_cache_infer(cache, inp, S, cval, stream);
+      if (status == N2W_OK) {
+        if (cache) {
+          status = n2w_cache_infer(cache, inp, S, cval, stream);
+        } else {
+          launch_oracle_cache(*problem, inp, S, o->input_min, o->input_extent, cval, stream);
+        }
+      }
+      if (status == N2W_OK && d_counters) {
+        unsigned long long* c = reinterpret_cast<unsigned long long*>(d_counters) + (mode == N2W_WALK_PREFIX ? 0 : 3);
+        launch_count_samples(needs, frc, ovf, S, c, stream);
+      }
       if (status == N2W_OK && mode == N2W_WALK_PREFIX) {
         // coarse value = A + needs * C; the combine kernel needs a continuation array
         status = n2w_wos_combine(cval, bnd, bnd, needs, S, ncv, res, 256, stream);

@@ -92,6 +92,20 @@ class Mesh:
         call("n2w_mesh_bounds", self._h, _ptr(b))
         return b[:3].copy(), b[3:].copy()
 
+    def closest_point_host(self, points: np.ndarray, threads: int = 0) -> dict:
+        """Host brute force over every triangle (the probes' validator)."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        n = len(pts)
+        d2 = np.empty(n, np.float32)
+        cp = np.empty((n, 3), np.float32)
+        ids = np.empty(n, np.int32)
+        call("n2w_mesh_closest_point_host", self._h, _ptr(pts), n, _ptr(d2), _ptr(cp), _ptr(ids), threads)
+        return {"distance2": d2, "closest": cp, "triangle_id": ids}
+
+    @property
+    def name(self) -> str:
+        return lib.n2w_mesh_name(self._h).decode()
+
     def degenerate_count(self, eps: float = 1e-20) -> int:
         out = C.c_int64()
         call("n2w_mesh_count_degenerate", self._h, C.c_float(eps), C.byref(out))

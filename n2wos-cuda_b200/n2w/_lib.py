@@ -96,6 +96,22 @@ class Nc2lmcOptions(C.Structure):
                 ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3), ("point_batch", C.c_int32)]
 
 
+class Nc2lmcCounters(C.Structure):
+    _fields_ = [(n, C.c_ulonglong) for n in
+                ("coarse_cache_queries", "coarse_forced", "coarse_overflow", "residual_cache_queries",
+                 "residual_forced", "residual_overflow")]
+
+
+class NcLabelOptions(C.Structure):
+    _fields_ = [("walks_per_point", C.c_int32), ("max_steps", C.c_int32), ("epsilon", C.c_float),
+                ("step_scale", C.c_float), ("seed", C.c_uint64), ("refresh_index", C.c_int32),
+                ("label_source", C.c_int32), ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3),
+                ("block_size", C.c_int32), ("reserved", C.c_int32)]
+
+
+N2W_LABEL_EXACT, N2W_LABEL_WOS = 0, 1
+N2W_SLICE_RULE_RENDER, N2W_SLICE_RULE_EVAL = 0, 1
+
 P = C.c_void_p
 I = C.c_int
 I64 = C.c_int64
@@ -117,6 +133,8 @@ _SIGS = {
     "n2w_mesh_copy_out": (I, [P, P, P]),
     "n2w_mesh_bounds": (I, [P, P]),
     "n2w_mesh_count_degenerate": (I, [P, C.c_float, C.POINTER(I64)]),
+    "n2w_mesh_closest_point_host": (I, [P, P, I64, P, P, P, I]),
+    "n2w_mesh_name": (C.c_char_p, [P]),
     "n2w_mesh_free": (None, [P]),
     "n2w_bvh_host_build": (I, [P, I, C.c_char_p, PP]),
     "n2w_bvh_host_stats": (I, [P, C.POINTER(BvhStats)]),
@@ -131,6 +149,7 @@ _SIGS = {
     "n2w_bvh_copy_layout": (I, [P, P, P]),
     "n2w_bvh_inside_device": (I, [P, P, I, P, P, I, P]),
     "n2w_slice_points": (I, [P, C.c_char_p, C.c_float, I, I, C.c_float, I, P, P]),
+    "n2w_slice_points_ex": (I, [P, P, C.c_char_p, C.c_float, I, I, C.c_float, I, I, P, P]),
     "n2w_problem_charges_seeded": (I, [I, C.c_float, C.c_float, C.c_uint64, C.POINTER(Problem)]),
     "n2w_problem_sinprod": (I, [C.c_float, I, C.POINTER(Problem)]),
     "n2w_problem_reference_mode": (I, [I, I, C.POINTER(Problem)]),
@@ -162,10 +181,20 @@ _SIGS = {
     "n2w_cache_save": (I, [P, C.c_char_p]),
     "n2w_cache_load": (I, [C.c_char_p, PP]),
     "n2w_sample_interior": (I, [P, P, P, I64, C.c_uint64, P, C.POINTER(I64), P]),
+    "n2w_sample_interior_ex": (I, [P, P, P, I64, C.c_uint64, P, C.POINTER(I64), C.POINTER(I64), P]),
     "n2w_map_to_unit": (I, [P, I64, P, P, P, P]),
     "n2w_nc_train": (I, [P, P, C.POINTER(Problem), C.POINTER(NcTrainOptions), P, P]),
     "n2w_nc2lmc_estimate": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,
                                 PointStats, P]),
+    "n2w_nc2lmc_estimate_ex": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,
+                                   PointStats, P, P]),
+    "n2w_nc_update_labels": (I, [P, C.POINTER(Problem), P, I64, C.POINTER(NcLabelOptions), PointStats, P, P, P,
+                                 P]),
+    "n2w_problem_exact_device": (I, [C.POINTER(Problem), P, I64, P, P]),
+    "n2w_oracle_cache_infer": (I, [C.POINTER(Problem), P, I64, P, P, P, P]),
+    "n2w_fill_unit_samples": (I, [C.POINTER(Problem), I64, C.c_uint64, C.c_uint32, P, P, P, P, P]),
+    "n2w_compare_accumulate": (I, [P, P, I64, P, P]),
+    "n2w_count_samples": (I, [P, P, P, I64, P, P]),
     "n2w_device_count": (I, [C.POINTER(I)]),
     "n2w_set_device": (I, [I]),
     "n2w_malloc": (I, [PP, C.c_size_t]),

@@ -28,10 +28,11 @@ def pytest_configure(config):
 
 def _ensure_built():
     lib = PKG / "lib" / "libn2w.so"
-    if not lib.exists():
-        sys.path.insert(0, str(PKG))
-        import build as pkg_build  # noqa: F401
+    sys.path.insert(0, str(PKG))
+    import build as pkg_build
 
+    tools = [PKG / "bin" / exe for exe in pkg_build.EXECUTABLES]
+    if not lib.exists() or not all(t.exists() for t in tools):
         pkg_build.build()
     orc = ROOT / "oracle" / "liboracle.so"
     if not orc.exists():
