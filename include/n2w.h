@@ -397,8 +397,9 @@ int n2w_cache_load(const char* path, n2w_cache** out);
 int n2w_sample_interior(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n,
                         uint64_t seed, n2w_vec3* d_points_out, int64_t* h_accepted_out,
                         n2w_stream_t stream);
-/* Same, also reporting the candidates drawn (*h_candidates_out, may be NULL);
- * accepted / candidates estimates the interior volume fraction of the box. */
+/* Same, also reporting *h_candidates_out (may be NULL): the candidates the n
+ * accepted points consumed, n * draws / hits over every draw of the launch, so
+ * n / *h_candidates_out estimates the interior volume fraction of the box. */
 int n2w_sample_interior_ex(const n2w_bvh* bvh, const float* box_lo, const float* box_hi, int64_t n,
                            uint64_t seed, n2w_vec3* d_points_out, int64_t* h_accepted_out,
                            int64_t* h_candidates_out, n2w_stream_t stream);
@@ -492,6 +493,74 @@ typedef struct n2w_nc_label_options {
 int n2w_nc_update_labels(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
                          const n2w_nc_label_options* options, n2w_point_stats accum, float* d_inputs,
                          float* d_targets, void* d_workspace, n2w_stream_t stream);
+
+/* ---- batched instances (one persistent launch) --------------------------- */
+/* A scene merges several BVHs into one device layout (indices rebased) so one
+ * launch can walk many meshes.  The BVHs may be destroyed afterwards.  No
+ * counterpart in the reference, which runs one problem per launch. */
+typedef struct n2w_scene n2w_scene;
+int n2w_scene_create(const n2w_bvh* const* bvhs, int count, n2w_scene** out);
+int n2w_scene_info(const n2w_scene* scene, int* mesh_count, int64_t* nodes, int64_t* triangles,
+                   int64_t* device_bytes);
+void n2w_scene_destroy(n2w_scene* scene);
+
+/* One PDE instance of a batch: plain WoS at point_count device points of scene
+ * mesh `mesh` for problem `problem` (index into the batch's problem array),
+ * walks_per_point walks each, Philox key `seed`.  Walks are keyed exactly as
+ * n2w_wos_estimate keys them, so an instance's estimates equal a single-problem
+ * call with the same seed up to the order of FP64 additions, whatever else the
+ * batch holds.  Results go to the instance's per-point accumulators. */
+typedef struct n2w_batch_item {
+  int32_t mesh;
+  int32_t problem;
+  const n2w_vec3* d_points;
+  int64_t point_count;
+  int32_t walks_per_point;
+  int32_t reserved;
+  uint64_t seed;
+  n2w_point_stats stats;
+} n2w_batch_item;
+
+/* Launch shape of a batch (the autotuner's search space). */
+typedef struct n2w_batch_tuning {
+  int32_t block_size;      /* walker threads per block: 64, 128 or 256 */
+  int32_t blocks_per_sm;   /* 0 = occupancy maximum */
+  int32_t chunk;           /* walks a lane takes per queue pop */
+  int32_t regen_threshold; /* waiting lanes that trigger walk updates */
+  int32_t reg_variant;     /* 0: 64 registers / 4 blocks per SM; 1: 80 registers / 3 blocks */
+  float ms;                /* autotuner: best time of this shape on the probe batch */
+} n2w_batch_tuning;
+
+typedef struct n2w_batch n2w_batch;
+/* Copies the problems and the instance table to the device.  options supplies
+ * max_steps, epsilon, step_scale, accumulate (0: each launch first zeroes every
+ * instance's accumulators) and the launch shape; walks_per_point and seed are
+ * per item. */
+int n2w_batch_create(const n2w_scene* scene, const n2w_problem* problems, int problem_count,
+                     const n2w_batch_item* items, int item_count, const n2w_walk_options* options,
+                     n2w_batch** out);
+int n2w_batch_info(const n2w_batch* batch, int64_t* total_points, int64_t* total_walks,
+                   n2w_walk_options* options_out, int* reg_variant_out);
+/* New Philox keys for every item (e.g. the next round of an adaptive estimate);
+ * synchronises the stream.  A captured graph picks them up. */
+int n2w_batch_set_seeds(n2w_batch* batch, const uint64_t* seeds, n2w_stream_t stream);
+/* One launch over every instance: memsets and kernels only, no allocation and
+ * no host synchronisation, so it can be captured into a CUDA graph.
+ * d_counters (device, may be NULL) receives run counters over all instances. */
+int n2w_batch_launch(n2w_batch* batch, n2w_walk_counters* d_counters, n2w_stream_t stream);
+/* Captures n2w_batch_launch on `stream` (not the legacy default stream) into a
+ * graph the batch owns; n2w_batch_graph_launch replays it. */
+int n2w_batch_capture_graph(n2w_batch* batch, n2w_walk_counters* d_counters, n2w_stream_t stream);
+int n2w_batch_graph_launch(n2w_batch* batch, n2w_stream_t stream);
+/* Times launch shapes on a probe batch (the first max(min(n,64), f*n) points of
+ * every item, scratch accumulators) and applies the fastest to the batch:
+ * threads per block x register budget, then chunk, then regeneration
+ * threshold.  Trials are copied to trials_out (up to trials_cap).  Drops a
+ * captured graph (capture again after tuning). */
+int n2w_batch_autotune(n2w_batch* batch, double sample_fraction, n2w_batch_tuning* best_out,
+                       n2w_batch_tuning* trials_out, int trials_cap, int* trials_count, n2w_stream_t stream);
+int n2w_batch_set_tuning(n2w_batch* batch, const n2w_batch_tuning* tuning, n2w_stream_t stream);
+void n2w_batch_destroy(n2w_batch* batch);
 
 /* ---- device utilities ---------------------------------------------------- */
 /* u(x) of the problem at n device points, evaluated in FP64 and stored as FP32. */

@@ -175,10 +175,10 @@ struct TraversalStats {
 template <bool kCount>
 __device__ __forceinline__ void traverse(const float4* __restrict__ nodes,
                                          const float4* __restrict__ tris, V3 p, ClosestHit& hit,
-                                         TraversalStats& st) {
+                                         TraversalStats& st, int32_t root = 0) {
   int2 stack[kTraversalStack];
   int sp = 0;
-  int32_t ref = 0;
+  int32_t ref = root;
   for (;;) {
     if (ref >= 0) {
       const float4* n = nodes + static_cast<size_t>(ref) * 8;

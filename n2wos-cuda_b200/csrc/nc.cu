@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <vector>
@@ -121,7 +122,13 @@ int n2w_sample_interior_ex(const n2w_bvh* bvh, const float* box_lo, const float*
     N2W_CUDA(cudaStreamSynchronize(stream));
     const int64_t acc = static_cast<int64_t>(std::min<unsigned long long>(c[1], static_cast<unsigned long long>(n)));
     if (h_accepted_out) *h_accepted_out = acc;
-    if (h_candidates_out) *h_candidates_out = static_cast<int64_t>(std::min<unsigned long long>(c[0], 1000ull * n + 1000000ull));
+    // Threads race past the n-th acceptance, so the raw counters overshoot; their
+    // ratio is still an unbiased acceptance estimate: report n / (hits / draws).
+    if (h_candidates_out) {
+      *h_candidates_out = c[1] ? static_cast<int64_t>(std::llround(static_cast<double>(n) * static_cast<double>(c[0]) /
+                                                                   static_cast<double>(c[1])))
+                               : static_cast<int64_t>(c[0]);
+    }
     if (acc < n) throw Error(N2W_EINTERNAL, "interior sampling gave up: the box holds too little interior");
   });
 }

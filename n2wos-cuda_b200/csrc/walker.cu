@@ -57,38 +57,35 @@ __device__ __forceinline__ float green_radius_fraction(float u) {
 
 __device__ __forceinline__ double shfl_xor_d(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
 
-// Dirichlet value at the terminal closest point.
-__device__ __forceinline__ float boundary_value(const WalkArgs& a, dev::V3 p) {
-  return problem_u<float>(a.problem, p.x, p.y, p.z);
-}
 
 // Source contribution of the ball B(x, R): (R^2/6) * f at the ball centre
 // (reference rule) or averaged over `source_samples` points drawn from the
 // ball's Green's function.  Sample 0 takes its radius fraction from word u2 of
 // the step's stream-0 draw and its direction from stream 1; samples k >= 1 use
 // stream 1 + k.
-__device__ __forceinline__ float ball_source(const WalkArgs& a, dev::V3 x, float R, uint64_t wid, int step,
-                                         uint32_t u2) {
+__device__ __forceinline__ float ball_source(const n2w_problem& pb, uint32_t k0, uint32_t k1, int source_center,
+                                             int source_samples, dev::V3 x, float R, uint64_t wid, int step,
+                                             uint32_t u2) {
   float f;
-  if (a.source_center) {
-    f = problem_f<float>(a.problem, x.x, x.y, x.z);
+  if (source_center) {
+    f = problem_f<float>(pb, x.x, x.y, x.z);
   } else {
     const float tfrac = green_radius_fraction(u01(u2));
     const U4 r2 = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
                                    static_cast<uint32_t>(step), 1u},
-                                a.k0, a.k1);
+                                k0, k1);
     const dev::V3 w = unit_sphere(r2.x, r2.y);
     const float rho = R * tfrac;
-    f = problem_f<float>(a.problem, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
-    for (int k = 1; k < a.source_samples; ++k) {
+    f = problem_f<float>(pb, x.x + rho * w.x, x.y + rho * w.y, x.z + rho * w.z);
+    for (int k = 1; k < source_samples; ++k) {
       const U4 rk = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
                                      static_cast<uint32_t>(step), 1u + static_cast<uint32_t>(k)},
-                                  a.k0, a.k1);
+                                  k0, k1);
       const float rk_rho = R * green_radius_fraction(u01(rk.x));
       const dev::V3 wk = unit_sphere(rk.y, rk.z);
-      f += problem_f<float>(a.problem, x.x + rk_rho * wk.x, x.y + rk_rho * wk.y, x.z + rk_rho * wk.z);
+      f += problem_f<float>(pb, x.x + rk_rho * wk.x, x.y + rk_rho * wk.y, x.z + rk_rho * wk.z);
     }
-    if (a.source_samples > 1) f *= 1.0f / static_cast<float>(a.source_samples);
+    if (source_samples > 1) f *= 1.0f / static_cast<float>(source_samples);
   }
   return (R * R) * (1.0f / 6.0f) * f;
 }
@@ -96,7 +93,8 @@ __device__ __forceinline__ float ball_source(const WalkArgs& a, dev::V3 x, float
 // Warp-collective flush of per-lane chunk accumulators into per-point FP64
 // totals: lanes are grouped by point id, each group is reduced by a shuffle
 // butterfly (non-members contribute zero) and its lowest lane issues the atomics.
-__device__ __forceinline__ void warp_flush(bool want, int64_t pid, double s, double s2, uint32_t n,
+template <bool kBatch>
+__device__ __forceinline__ void warp_flush(bool want, int64_t pid, int inst, double s, double s2, uint32_t n,
                                            uint64_t steps, uint32_t forced, const WalkArgs& a) {
   unsigned pending = __ballot_sync(0xffffffffu, want);
   const int lane = threadIdx.x & 31;
@@ -116,7 +114,19 @@ __device__ __forceinline__ void warp_flush(bool want, int64_t pid, double s, dou
       vn += __shfl_xor_sync(0xffffffffu, vn, o);
       vf += __shfl_xor_sync(0xffffffffu, vf, o);
     }
-    if (lane == leader) {
+    if (kBatch) {
+      // pid is the global point index; the leader's instance owns the accumulators.
+      const int li = __shfl_sync(0xffffffffu, inst, leader);
+      if (lane == leader) {
+        const BatchInst& I = a.insts[li];
+        const int64_t q = lp - I.point_base;
+        atomicAdd(I.sum + q, vs);
+        atomicAdd(I.sum_sq + q, vs2);
+        atomicAdd(I.count + q, vn);
+        atomicAdd(reinterpret_cast<unsigned long long*>(I.steps) + q, vst);
+        atomicAdd(I.forced + q, vf);
+      }
+    } else if (lane == leader) {
       atomicAdd(a.sum + lp, vs);
       atomicAdd(a.sum_sq + lp, vs2);
       atomicAdd(a.count + lp, vn);
@@ -226,15 +236,18 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
 //    warp returns to Phase A once `regen` lanes are waiting (or none is busy),
 //    so the walk updates run for many lanes at once and no lane waits for
 //    another lane's whole traversal.
-template <int kOut, int kWalk>
-__global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_kernel(const __grid_constant__ WalkArgs a) {
+template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks>
+__global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(const __grid_constant__ WalkArgs a) {
+  static_assert(!kBatch || (kOut == kOutStats && kWalk == N2W_WALK_PURE),
+                "batched launches run plain walks into per-point statistics");
   const int lane = threadIdx.x & 31;
   const uint64_t t_start = (a.deadline_ns > 0) ? global_ns() : 0;
 
   bool alive = false;     // a walk is in progress on this lane
   bool querying = false;  // its closest-point query is in flight
   bool exhausted = false; // the global queue has no chunk left for this lane
-  int64_t pid = -1;
+  int64_t pid = -1;  // global point index
+  int inst = 0;      // batched launches: instance of the current chunk
   int walk = 0, walk_end = 0;
   dev::V3 x = dev::v3(0, 0, 0), xm = dev::v3(0, 0, 0);
   float src = 0.0f, am = 0.0f;
@@ -257,6 +270,17 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
   uint32_t c_walks = 0, c_steps = 0, c_queries = 0, c_nodes = 0, c_tris = 0, c_overflow = 0, c_forced = 0,
            c_timeout = 0;
 
+  // Per-instance parameters: kernel arguments for a single problem, the
+  // instance table (L1-resident) for batched launches.
+  auto problem_of = [&]() -> const n2w_problem& {
+    if constexpr (kBatch) return *a.insts[inst].problem;
+    else return a.problem;
+  };
+  auto start_point = [&]() -> n2w_vec3 {
+    if constexpr (kBatch) return a.insts[inst].points[pid - a.insts[inst].point_base];
+    else return a.points[pid];
+  };
+
   for (;;) {
     // ================= Phase A =================
     // (1) deadline: abandon the current walk and stop taking work.
@@ -277,7 +301,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
       const bool forced = rel >= a.max_steps;
       const bool stop = d <= a.eps || forced || !isfinite(d) || hit.id == INT32_MAX;
       if (stop || (kWalk == N2W_WALK_PREFIX && step >= a.depth_m)) {
-        const float value = stop ? src + boundary_value(a, hit.cp) : src;
+        const float value = stop ? src + problem_u<float>(problem_of(), hit.cp.x, hit.cp.y, hit.cp.z) : src;
         ++c_walks;
         c_steps += static_cast<uint32_t>(step);
         c_forced += forced ? 1u : 0u;
@@ -314,7 +338,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
         ++walk;
         if (walk < walk_end) {
           // next walk of the same chunk: same point, cached first query
-          const n2w_vec3 p0 = a.points[pid];
+          const n2w_vec3 p0 = start_point();
           x = dev::v3(p0.x, p0.y, p0.z);
           src = 0.0f;
           step = 0;
@@ -342,15 +366,31 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
         cont0 = step;
       }
       const float R = a.step_scale * d;
+      uint32_t k0 = a.k0, k1 = a.k1;
+      if constexpr (kBatch) {
+        k0 = a.insts[inst].k0;
+        k1 = a.insts[inst].k1;
+      }
       const U4 r = philox4x32_10(U4{static_cast<uint32_t>(wid), static_cast<uint32_t>(wid >> 32),
                                     static_cast<uint32_t>(step), 0u},
-                                 a.k0, a.k1);
+                                 k0, k1);
       const dev::V3 dir = unit_sphere(r.x, r.y);
-      if (a.has_source) src += ball_source(a, x, R, wid, step, r.z);
+      if constexpr (kBatch) {
+        const BatchInst& I = a.insts[inst];
+        if (I.has_source) src += ball_source(*I.problem, k0, k1, I.source_center, I.source_samples, x, R, wid, step, r.z);
+      } else {
+        if (a.has_source) src += ball_source(a.problem, k0, k1, a.source_center, a.source_samples, x, R, wid, step, r.z);
+      }
       const int prev_slot = hit.slot;
       const dev::V3 xn = dev::v3(x.x + R * dir.x, x.y + R * dir.y, x.z + R * dir.z);
-      if (!(xn.x >= a.box_lo[0] && xn.x <= a.box_hi[0] && xn.y >= a.box_lo[1] && xn.y <= a.box_hi[1] &&
-            xn.z >= a.box_lo[2] && xn.z <= a.box_hi[2])) {
+      const float* blo = a.box_lo;
+      const float* bhi = a.box_hi;
+      if constexpr (kBatch) {
+        blo = a.insts[inst].box_lo;
+        bhi = a.insts[inst].box_hi;
+      }
+      if (!(xn.x >= blo[0] && xn.x <= bhi[0] && xn.y >= blo[1] && xn.y <= bhi[1] && xn.z >= blo[2] &&
+            xn.z <= bhi[2])) {
         // A walk from an interior point stays inside the mesh; leaving the
         // domain box means the start point was outside (a misclassified sample).
         // Stop it as forced, scored at the current closest point, instead of
@@ -367,15 +407,20 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
       hit.cp = x;
       dev::test_slot(a.tris, prev_slot, x, hit);
       ++c_tris;
-      if (a.grid.slots) {
-        const int sg = dev::seed_slot(a.grid, x);
+      const dev::SeedGrid& grid = [&]() -> const dev::SeedGrid& {
+        if constexpr (kBatch) return a.insts[inst].grid;
+        else return a.grid;
+      }();
+      if (grid.slots) {
+        const int sg = dev::seed_slot(grid, x);
         if (sg != prev_slot) {
           dev::test_slot(a.tris, sg, x, hit);
           ++c_tris;
         }
       }
       tv.sp = 0;
-      tv.ref = 0;
+      if constexpr (kBatch) tv.ref = a.insts[inst].root;
+      else tv.ref = 0;
       tv.leaf_cur = tv.leaf_end = 0;
       querying = true;
     }
@@ -383,7 +428,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
     //     exit test below, so nothing accumulated is ever dropped.
     if (kOut == kOutStats) {
       const bool want = !alive && walk >= walk_end && acc_n > 0;
-      warp_flush(want, pid, acc_s, acc_s2, acc_n, acc_steps, acc_forced, a);
+      warp_flush<kBatch>(want, pid, inst, acc_s, acc_s2, acc_n, acc_steps, acc_forced, a);
       if (want) {
         acc_s = acc_s2 = 0.0;
         acc_n = acc_forced = acc_steps = 0;
@@ -400,17 +445,39 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kWalkerMinBlocks) walker_ke
       if (need) {
         const unsigned long long c = base + __popc(need_mask & ((1u << lane) - 1u));
         if (c < static_cast<unsigned long long>(a.total_chunks)) {
-          pid = static_cast<int64_t>(c / static_cast<unsigned long long>(a.chunks_per_point));
-          walk = static_cast<int>((c % static_cast<unsigned long long>(a.chunks_per_point)) * a.chunk);
-          walk_end = min(walk + a.chunk, a.walks_per_point);
-          const n2w_vec3 p0 = a.points[pid];
+          int64_t lpid;  // point index within the instance (keys its walks' random streams)
+          int wpp;
+          if constexpr (kBatch) {
+            // Instance of chunk c: the last one whose chunk_base <= c.
+            int lo = 0, hi = a.n_insts - 1;
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (static_cast<unsigned long long>(a.insts[mid].chunk_base) <= c) lo = mid;
+              else hi = mid - 1;
+            }
+            inst = lo;
+            const BatchInst& I = a.insts[inst];
+            const unsigned long long lc = c - static_cast<unsigned long long>(I.chunk_base);
+            const unsigned long long cpp = static_cast<unsigned long long>(I.chunks_per_point);
+            lpid = static_cast<int64_t>(lc / cpp);
+            wpp = I.walks_per_point;
+            walk = static_cast<int>((lc % cpp) * a.chunk);
+            pid = I.point_base + lpid;
+          } else {
+            lpid = static_cast<int64_t>(c / static_cast<unsigned long long>(a.chunks_per_point));
+            wpp = a.walks_per_point;
+            walk = static_cast<int>((c % static_cast<unsigned long long>(a.chunks_per_point)) * a.chunk);
+            pid = lpid;
+          }
+          walk_end = min(walk + a.chunk, wpp);
+          const n2w_vec3 p0 = start_point();
           x = dev::v3(p0.x, p0.y, p0.z);
           src = 0.0f;
           step = 0;
           cont0 = 0;
           has_xm = false;
           w_overflow = false;
-          wid = static_cast<uint64_t>(pid) * static_cast<uint64_t>(a.walks_per_point) + static_cast<uint64_t>(walk);
+          wid = static_cast<uint64_t>(lpid) * static_cast<uint64_t>(wpp) + static_cast<uint64_t>(walk);
           const float4 cc = __ldg(a.first_cpd + pid);
           const int2 ii = __ldg(a.first_ids + pid);
           hit.cp = dev::v3(cc.x, cc.y, cc.z);
@@ -494,6 +561,41 @@ __global__ void __launch_bounds__(256) first_query_kernel(const float4* __restri
   }
 }
 
+// First queries of a batched launch: point i belongs to the last instance whose
+// point_base <= i; its query starts at that instance's root in the merged scene.
+__global__ void __launch_bounds__(256) first_query_batch_kernel(const __grid_constant__ WalkArgs a, int64_t n,
+                                                                float4* __restrict__ cpd, int2* __restrict__ ids) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int lo = 0, hi = a.n_insts - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.insts[mid].point_base <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchInst& I = a.insts[lo];
+  const n2w_vec3 pt = I.points[i - I.point_base];
+  const dev::V3 p = dev::v3(pt.x, pt.y, pt.z);
+  dev::ClosestHit hit;
+  hit.d2 = FLT_MAX;
+  hit.id = INT32_MAX;
+  hit.slot = -1;
+  hit.cp = p;
+  dev::TraversalStats st{0, 0, 0};
+  if (I.grid.slots) {
+    dev::test_slot(a.tris, dev::seed_slot(I.grid, p), p, hit);
+    ++st.tri_tests;
+  }
+  dev::traverse<true>(a.nodes, a.tris, p, hit, st, I.root);
+  cpd[i] = make_float4(hit.cp.x, hit.cp.y, hit.cp.z, hit.d2);
+  ids[i] = make_int2(hit.id, hit.slot);
+  if (a.counters) {
+    atomicAdd(&a.counters->node_visits, static_cast<unsigned long long>(st.node_visits));
+    atomicAdd(&a.counters->tri_tests, static_cast<unsigned long long>(st.tri_tests));
+    if (st.overflow) atomicAdd(&a.counters->overflow, 1ull);
+  }
+}
+
 // ---- per-sample reduction and 2LMC combination ------------------------------
 __global__ void reduce_samples_kernel(const float* __restrict__ values, const int* __restrict__ steps,
                                       const int* __restrict__ forced, int64_t points, int W,
@@ -556,9 +658,9 @@ __global__ void combine_kernel(const float* __restrict__ cache, const float* __r
 // ---- host side -----------------------------------------------------------
 namespace {
 
-template <int kOut, int kWalk>
+template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks>
 void launch_walker(const WalkArgs& a, int block, int blocks_per_sm, cudaStream_t stream) {
-  auto kern = walker_kernel<kOut, kWalk>;
+  auto kern = walker_kernel<kOut, kWalk, kBatch, kMinBlocks>;
   int occ = 0;
   N2W_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, 0));
   if (occ < 1) occ = 1;
@@ -572,6 +674,35 @@ void launch_walker(const WalkArgs& a, int block, int blocks_per_sm, cudaStream_t
 }
 
 }  // namespace
+
+void launch_first_query_batch(const WalkArgs& a, int64_t total_points, float4* cpd, int2* ids, cudaStream_t s) {
+  if (total_points == 0) return;
+  const int block = 256;
+  first_query_batch_kernel<<<static_cast<unsigned>((total_points + block - 1) / block), block, 0, s>>>(
+      a, total_points, cpd, ids);
+  N2W_CUDA(cudaGetLastError());
+}
+
+// Two register budgets for the batched walker: 64 registers (4 resident
+// 256-thread blocks per SM, some spills of the per-instance state) or 80
+// registers (3 blocks, fewer spills); the autotuner picks one per workload.
+void launch_walker_batch(const WalkArgs& a, int block, int blocks_per_sm, int reg_variant, cudaStream_t s) {
+  if (a.total_chunks == 0) return;
+  if (reg_variant == 1) launch_walker<kOutStats, N2W_WALK_PURE, true, 3>(a, block, blocks_per_sm, s);
+  else launch_walker<kOutStats, N2W_WALK_PURE, true, 4>(a, block, blocks_per_sm, s);
+}
+
+int walker_batch_occupancy(int block, int reg_variant) {
+  int occ = 0;
+  if (reg_variant == 1) {
+    N2W_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, walker_kernel<kOutStats, N2W_WALK_PURE, true, 3>,
+                                                            block, 0));
+  } else {
+    N2W_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, walker_kernel<kOutStats, N2W_WALK_PURE, true, 4>,
+                                                            block, 0));
+  }
+  return occ;
+}
 
 void validate_walk_options(const n2w_walk_options& o) {
   N2W_REQUIRE(o.walks_per_point > 0, "walks_per_point must be positive");

@@ -1,6 +1,7 @@
 // Kernel argument block of the persistent walker (walker.cu).
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "geom.cuh"
@@ -19,6 +20,28 @@ constexpr int kWalkerMinBlocks = 4;
 constexpr int kDefaultWalkerThreads = 128;
 constexpr int kDefaultChunk = 8;
 constexpr int kDefaultRegen = 12;
+
+// One instance of a batched launch: its geometry inside the merged scene, its
+// problem, its points and accumulators, and its slice of the global chunk queue.
+struct alignas(16) BatchInst {
+  const n2w_vec3* points;       // this instance's points
+  const n2w_problem* problem;   // device copy of its problem
+  double* sum;                  // per-point accumulators (local point index)
+  double* sum_sq;
+  uint32_t* count;
+  uint64_t* steps;
+  uint32_t* forced;
+  int64_t point_base;           // first global point index (first-query cache)
+  int64_t point_count;
+  int64_t chunk_base;           // first global chunk of this instance
+  int64_t chunks_per_point;
+  dev::SeedGrid grid;           // slots already rebased into the merged scene
+  float box_lo[3], box_hi[3];   // domain box (walks never leave it)
+  int32_t walks_per_point;
+  int32_t root;                 // root node of this instance's mesh in the scene
+  uint32_t k0, k1;              // Philox key of the instance
+  int32_t has_source, source_center, source_samples, pad;
+};
 
 struct WalkArgs {
   const float4* nodes;
@@ -65,8 +88,20 @@ struct WalkArgs {
   // scratch
   unsigned long long* queue;
   n2w_walk_counters* counters;
+  // batched launches: instance table sorted by chunk_base / point_base
+  const BatchInst* insts;
+  int n_insts;
 };
 
 dev::SeedGrid seed_grid_of(const n2w_bvh& b);
+void validate_problem(const n2w_problem& p);
+void validate_walk_options(const n2w_walk_options& o);
+
+// Batched launches (walker.cu): per-point first queries of every instance, and
+// the persistent walker over the concatenated chunk queue of all instances.
+// reg_variant 0: 64 registers / 4 blocks per SM; 1: 80 registers / 3 blocks.
+void launch_first_query_batch(const WalkArgs& a, int64_t total_points, float4* cpd, int2* ids, cudaStream_t s);
+void launch_walker_batch(const WalkArgs& a, int block, int blocks_per_sm, int reg_variant, cudaStream_t s);
+int walker_batch_occupancy(int block, int reg_variant);
 
 }  // namespace n2w

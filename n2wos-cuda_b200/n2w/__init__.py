@@ -20,6 +20,7 @@ __all__ = [
     "problem_sinprod", "problem_reference", "problem_from_name", "walk_options", "wos_estimate",
     "N2wError", "LIB_PATH", "EXPORTED", "N2W_BC", "device_count", "device_summary", "runtime_version",
     "N2W_SOURCE_BALL", "N2W_SOURCE_CENTER", "N2W_WALK_PURE", "N2W_WALK_PREFIX", "N2W_WALK_RESIDUAL",
+    "Scene", "Batch",
 ]
 
 
@@ -442,6 +443,129 @@ def wos_estimate(bvh: Bvh, problem: Problem, points: np.ndarray | DeviceBuffer, 
         raw = dcount.download(np.uint64, 8)
         cnt = dict(zip([f for f, _ in WalkCounters._fields_], (int(v) for v in raw)))
     return res, cnt
+
+
+class Scene:
+    """Several BVHs merged into one device layout for batched launches."""
+
+    def __init__(self, bvhs):
+        arr = (C.c_void_p * len(bvhs))(*[b.handle for b in bvhs])
+        h = C.c_void_p()
+        call("n2w_scene_create", arr, len(bvhs), C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        m, nodes, tris, by = C.c_int(), C.c_int64(), C.c_int64(), C.c_int64()
+        call("n2w_scene_info", self._h, C.byref(m), C.byref(nodes), C.byref(tris), C.byref(by))
+        return {"meshes": m.value, "nodes": nodes.value, "triangles": tris.value, "device_bytes": by.value}
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.n2w_scene_destroy(self._h)
+            self._h = None
+
+
+class Batch:
+    """Many plain-WoS instances in one persistent launch (optionally a CUDA graph).
+
+    ``instances`` is a list of dicts with keys mesh, problem (index), points
+    (N x 3 array), walks_per_point and seed.  Per-instance statistics are kept
+    in device buffers owned by the batch."""
+
+    def __init__(self, scene: Scene, problems, instances, options: WalkOptions | None = None):
+        from ._lib import BatchItem
+
+        self.scene = scene
+        self.options = options or walk_options()
+        self.points = []
+        self.stats = []
+        items = (BatchItem * len(instances))()
+        for k, inst in enumerate(instances):
+            pts = np.ascontiguousarray(inst["points"], np.float32).reshape(-1, 3)
+            dp = DeviceBuffer.from_array(pts) if len(pts) else DeviceBuffer(12)
+            st = PointStatsBuffers.allocate(max(len(pts), 1))
+            st.n = len(pts)
+            self.points.append(dp)
+            self.stats.append(st)
+            items[k].mesh = inst["mesh"]
+            items[k].problem = inst["problem"]
+            items[k].d_points = dp.ptr
+            items[k].point_count = len(pts)
+            items[k].walks_per_point = inst["walks_per_point"]
+            items[k].seed = inst.get("seed", 12345 + k)
+            items[k].stats = st.struct()
+        self._problems = (Problem * len(problems))(*problems)
+        h = C.c_void_p()
+        call("n2w_batch_create", scene.handle, self._problems, len(problems), items, len(instances),
+             C.byref(self.options), C.byref(h))
+        self._h = h
+        self.counters = DeviceBuffer(C.sizeof(WalkCounters))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def launch(self, stream: Stream | None = None, counters: bool = True):
+        call("n2w_batch_launch", self._h, self.counters.ptr if counters else None,
+             stream.handle if stream else None)
+
+    def capture_graph(self, stream: Stream):
+        call("n2w_batch_capture_graph", self._h, self.counters.ptr, stream.handle)
+
+    def graph_launch(self, stream: Stream):
+        call("n2w_batch_graph_launch", self._h, stream.handle)
+
+    def set_seeds(self, seeds, stream: Stream | None = None):
+        arr = (C.c_uint64 * len(seeds))(*[int(s) for s in seeds])
+        call("n2w_batch_set_seeds", self._h, arr, stream.handle if stream else None)
+
+    def autotune(self, sample_fraction: float = 0.0625, stream: Stream | None = None) -> dict:
+        from ._lib import BatchTuning
+
+        best = BatchTuning()
+        trials = (BatchTuning * 64)()
+        n = C.c_int()
+        call("n2w_batch_autotune", self._h, C.c_double(sample_fraction), C.byref(best), trials, 64, C.byref(n),
+             stream.handle if stream else None)
+        fields = [f for f, _ in BatchTuning._fields_]
+
+        def as_dict(t):
+            return {f: getattr(t, f) for f in fields}
+
+        return {"best": as_dict(best), "trials": [as_dict(trials[i]) for i in range(n.value)]}
+
+    def set_tuning(self, tuning: dict, stream: Stream | None = None):
+        from ._lib import BatchTuning
+
+        t = BatchTuning()
+        for k, v in tuning.items():
+            if k != "ms":
+                setattr(t, k, int(v))
+        call("n2w_batch_set_tuning", self._h, C.byref(t), stream.handle if stream else None)
+
+    def info(self) -> dict:
+        tp, tw, rv = C.c_int64(), C.c_int64(), C.c_int()
+        o = WalkOptions()
+        call("n2w_batch_info", self._h, C.byref(tp), C.byref(tw), C.byref(o), C.byref(rv))
+        return {"total_points": tp.value, "total_walks": tw.value, "block_size": o.block_size, "chunk": o.chunk,
+                "regen_threshold": o.regen_threshold, "reg_variant": rv.value}
+
+    def results(self, stream: Stream | None = None):
+        call("n2w_stream_sync", stream.handle if stream else None)
+        return [st.download(stream) if st.n else None for st in self.stats]
+
+    def run_counters(self) -> dict:
+        raw = self.counters.download(np.uint64, 8)
+        return dict(zip([f for f, _ in WalkCounters._fields_], (int(v) for v in raw)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.n2w_batch_destroy(self._h)
+            self._h = None
 
 
 def cache_config(**overrides):

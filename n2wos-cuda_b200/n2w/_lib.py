@@ -109,6 +109,17 @@ class NcLabelOptions(C.Structure):
                 ("block_size", C.c_int32), ("reserved", C.c_int32)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("mesh", C.c_int32), ("problem", C.c_int32), ("d_points", C.c_void_p), ("point_count", C.c_int64),
+                ("walks_per_point", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_uint64),
+                ("stats", PointStats)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk", C.c_int32),
+                ("regen_threshold", C.c_int32), ("reg_variant", C.c_int32), ("ms", C.c_float)]
+
+
 N2W_LABEL_EXACT, N2W_LABEL_WOS = 0, 1
 N2W_SLICE_RULE_RENDER, N2W_SLICE_RULE_EVAL = 0, 1
 
@@ -195,6 +206,18 @@ _SIGS = {
     "n2w_fill_unit_samples": (I, [C.POINTER(Problem), I64, C.c_uint64, C.c_uint32, P, P, P, P, P]),
     "n2w_compare_accumulate": (I, [P, P, I64, P, P]),
     "n2w_count_samples": (I, [P, P, P, I64, P, P]),
+    "n2w_scene_create": (I, [C.POINTER(C.c_void_p), I, PP]),
+    "n2w_scene_info": (I, [P, C.POINTER(I), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
+    "n2w_scene_destroy": (None, [P]),
+    "n2w_batch_create": (I, [P, C.POINTER(Problem), I, C.POINTER(BatchItem), I, C.POINTER(WalkOptions), PP]),
+    "n2w_batch_info": (I, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(WalkOptions), C.POINTER(I)]),
+    "n2w_batch_set_seeds": (I, [P, C.POINTER(C.c_uint64), P]),
+    "n2w_batch_launch": (I, [P, P, P]),
+    "n2w_batch_capture_graph": (I, [P, P, P]),
+    "n2w_batch_graph_launch": (I, [P, P]),
+    "n2w_batch_autotune": (I, [P, C.c_double, C.POINTER(BatchTuning), C.POINTER(BatchTuning), I, C.POINTER(I), P]),
+    "n2w_batch_set_tuning": (I, [P, C.POINTER(BatchTuning), P]),
+    "n2w_batch_destroy": (None, [P]),
     "n2w_device_count": (I, [C.POINTER(I)]),
     "n2w_set_device": (I, [I]),
     "n2w_malloc": (I, [PP, C.c_size_t]),
