@@ -488,6 +488,8 @@ class Batch:
             pts = np.ascontiguousarray(inst["points"], np.float32).reshape(-1, 3)
             dp = DeviceBuffer.from_array(pts) if len(pts) else DeviceBuffer(12)
             st = PointStatsBuffers.allocate(max(len(pts), 1))
+            for buf in (st.sum, st.sum_sq, st.count, st.steps, st.forced):
+                buf.zero()  # launches with accumulate=1 add to these
             st.n = len(pts)
             self.points.append(dp)
             self.stats.append(st)
