@@ -562,6 +562,80 @@ int n2w_batch_autotune(n2w_batch* batch, double sample_fraction, n2w_batch_tunin
 int n2w_batch_set_tuning(n2w_batch* batch, const n2w_batch_tuning* tuning, n2w_stream_t stream);
 void n2w_batch_destroy(n2w_batch* batch);
 
+/* ---- serving loop (continuous batching) ---------------------------------- */
+/* A device-resident request loop: meshes (as one scene), problems and walker
+ * buffers stay on the GPU; requests of uneven point counts are admitted while
+ * a device pool allocated at start-up has room, and every tick runs ONE
+ * persistent walker launch over all in-flight requests, so requests that
+ * arrive while others run join the next launch.  Each request runs sweeps of
+ * walks until the maximum per-point standard error is <= its target (or its
+ * walk cap).  A request's result does not depend on the other requests (up
+ * to the order of FP64 additions).  No counterpart in the reference. */
+#define N2W_REQUEST_PENDING 0 /* waiting for admission (pool memory / in-flight slots) */
+#define N2W_REQUEST_ACTIVE 1  /* admitted, walking */
+#define N2W_REQUEST_DONE 2    /* target standard error reached */
+#define N2W_REQUEST_CAPPED 3  /* stopped at max_walks_per_point */
+#define N2W_REQUEST_FAILED 4
+
+typedef struct n2w_server_options {
+  int64_t pool_bytes;      /* device pool for requests; 0 = pool_fraction of free memory */
+  float pool_fraction;     /* used when pool_bytes == 0 (default 0.25) */
+  int32_t max_inflight;    /* requests admitted at once (default 256) */
+  int64_t tick_walks;      /* walks shared out per tick (default 2^21) */
+  int32_t max_steps;       /* walk cap (default 256) */
+  float epsilon;           /* stopping shell (default 1e-3) */
+  float step_scale;        /* default 0.999 */
+  int32_t block_size;      /* walker threads per block (default 256) */
+  int32_t regen_threshold; /* default 8 */
+} n2w_server_options;
+
+typedef struct n2w_request {
+  int32_t mesh;                /* index into the server's meshes */
+  int32_t problem;             /* index into the server's problems */
+  int64_t point_count;
+  float target_stderr;         /* stop when max over points of the standard error <= this */
+  int32_t min_walks_per_point; /* first sweep size floor (>= 32 walks are used) */
+  int32_t max_walks_per_point; /* walk cap per point */
+  uint64_t seed;
+} n2w_request;
+
+typedef struct n2w_request_info {
+  int32_t state;            /* N2W_REQUEST_* */
+  int32_t sweeps;
+  int64_t walks_per_point;  /* walks each point received */
+  int64_t ticks;            /* launches the request took part in */
+  float max_stderr;         /* max per-point standard error at the end */
+  double queue_seconds;     /* submission -> admission */
+  double latency_seconds;   /* submission -> result ready */
+} n2w_request_info;
+
+typedef struct n2w_server_stats {
+  int64_t submitted, completed, inflight, pending, peak_inflight;
+  int64_t ticks, walks, walk_steps, overflow;
+  int64_t pool_bytes, pool_used, peak_pool_bytes;
+} n2w_server_stats;
+
+typedef struct n2w_server n2w_server;
+int n2w_server_options_default(n2w_server_options* out);
+/* Builds the scene from the BVHs (which may be destroyed afterwards), copies
+ * the problems, allocates the pool and starts the worker thread on the
+ * current device. */
+int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_problem* problems, int problem_count,
+                      const n2w_server_options* options, n2w_server** out);
+/* Thread-safe.  Copies the host points (3 * point_count floats).  Requests
+ * larger than the whole pool fail with N2W_ENOMEM. */
+int n2w_server_submit(n2w_server* server, const n2w_request* request, const float* h_points, int64_t* id_out);
+int n2w_server_poll(n2w_server* server, int64_t id, int* state_out);
+/* Blocks until the request finishes (timeout_seconds < 0: no limit; on
+ * timeout N2W_ETIMEOUT and the request stays), then copies per-point means and
+ * standard errors (point_count doubles each; either may be NULL) and releases
+ * the request. */
+int n2w_server_wait(n2w_server* server, int64_t id, double timeout_seconds, double* h_mean, double* h_stderr,
+                    n2w_request_info* info);
+int n2w_server_get_stats(n2w_server* server, n2w_server_stats* out);
+/* Stops the worker (unfinished requests fail) and frees everything. */
+void n2w_server_destroy(n2w_server* server);
+
 /* ---- device utilities ---------------------------------------------------- */
 /* u(x) of the problem at n device points, evaluated in FP64 and stored as FP32. */
 int n2w_problem_exact_device(const n2w_problem* problem, const n2w_vec3* d_points, int64_t n, float* d_u_out,

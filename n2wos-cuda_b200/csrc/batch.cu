@@ -30,26 +30,8 @@
 #include "internal.hpp"
 #include "philox.cuh"
 #include "problem.cuh"
+#include "scene.hpp"
 #include "walker.cuh"
-
-struct n2w_scene {
-  n2w::Node4* d_nodes = nullptr;
-  n2w::TriRec* d_tris = nullptr;
-  int* d_slots = nullptr;
-  int64_t nodes = 0, tris = 0, slots = 0;
-  struct MeshEntry {
-    int32_t root = 0;
-    int64_t node_off = 0, tri_off = 0, slot_off = -1;
-    float seed_lo[3] = {0, 0, 0};
-    float seed_h = 0.0f;
-    int seed_n = 0;
-    float box_lo[3] = {-1.0e30f, -1.0e30f, -1.0e30f};
-    float box_hi[3] = {1.0e30f, 1.0e30f, 1.0e30f};
-    int64_t triangles = 0;
-  };
-  std::vector<MeshEntry> meshes;
-  int device = 0;
-};
 
 struct n2w_batch {
   const n2w_scene* scene = nullptr;
@@ -127,10 +109,8 @@ void build_instances(n2w_batch& b) {
   int64_t pbase = 0, cbase = 0;
   for (int k = 0; k < b.n_items; ++k) {
     const n2w_batch_item& it = b.items[k];
-    const auto& m = sc.meshes[it.mesh];
     BatchInst& I = b.h_insts[k];
     I.points = it.d_points;
-    I.problem = b.d_problems + it.problem;
     I.sum = it.stats.d_sum;
     I.sum_sq = it.stats.d_sum_sq;
     I.count = it.stats.d_count;
@@ -141,22 +121,10 @@ void build_instances(n2w_batch& b) {
     I.chunk_base = cbase;
     I.chunks_per_point = (it.walks_per_point + chunk - 1) / chunk;
     I.walks_per_point = it.walks_per_point;
-    I.root = m.root;
-    I.grid.slots = m.slot_off >= 0 ? sc.d_slots + m.slot_off : nullptr;
-    I.grid.lo_x = m.seed_lo[0];
-    I.grid.lo_y = m.seed_lo[1];
-    I.grid.lo_z = m.seed_lo[2];
-    I.grid.inv_h = m.seed_h > 0.0f ? 1.0f / m.seed_h : 0.0f;
-    I.grid.n = m.seed_n;
-    for (int a = 0; a < 3; ++a) {
-      I.box_lo[a] = m.box_lo[a];
-      I.box_hi[a] = m.box_hi[a];
-    }
+    set_instance_geometry(I, sc, it.mesh);
+    set_instance_problem(I, b.problems[it.problem], b.d_problems + it.problem);
     philox_key(it.seed, 0u, I.k0, I.k1);
-    const n2w_problem& pb = b.problems[it.problem];
-    I.has_source = problem_has_source(pb) ? 1 : 0;
-    I.source_center = pb.source_sampling == N2W_SOURCE_CENTER ? 1 : 0;
-    I.source_samples = pb.source_samples > 1 ? pb.source_samples : 1;
+    I.wid_base = 0;
     pbase += it.point_count;
     cbase += it.point_count * I.chunks_per_point;
   }

@@ -1,0 +1,650 @@
+// Serving loop: continuous batching of Walk-on-Spheres evaluation requests on
+// one GPU.
+//
+// Requests (a mesh, a boundary problem, host points, a target standard error)
+// are submitted from any host thread.  A worker thread owns the GPU side:
+//
+//  * Admission by device memory.  One device pool is allocated when the server
+//    starts; a request is admitted when its points and per-point accumulators
+//    fit in the pool (first fit) and the in-flight limit allows it, so the
+//    request path never calls cudaMalloc.  Requests larger than the whole
+//    pool are refused at submission.
+//  * Ticks.  Each tick is ONE persistent walker launch over every in-flight
+//    request (the batched walker of batch.cu): a walk budget is shared out by
+//    water-filling, each request contributes its next range of points with
+//    its current sweep's walks per point, and requests admitted during a tick
+//    join the next one.  Small requests therefore overlap with large ones
+//    instead of queueing behind them.
+//  * Adaptive sweeps.  A sweep gives every point of a request the same number
+//    of walks; after each sweep the maximum per-point standard error is
+//    reduced on the device and the next sweep is sized from it
+//    (N_needed = N_done * (stderr / target)^2, plus 10 %), until the target or
+//    the walk cap is met.
+//  * Determinism.  Walk w of point p in sweep s of a request is keyed by
+//    (request seed, s; p * walks_per_point + w), whatever range or tick ran it,
+//    and sweep sizes depend only on the request's own statistics, so a
+//    request's estimates are the same alone and in any mix, up to the order of
+//    FP64 additions.
+//
+// The reference has no serving loop (it evaluates one point set per process);
+// the walk itself is the reference's (src/cuda/cubql_bvh.cu:1323-1357).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "internal.hpp"
+#include "philox.cuh"
+#include "problem.cuh"
+#include "scene.hpp"
+#include "walker.cuh"
+
+namespace n2w {
+namespace {
+
+int64_t now_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// Max over points of the standard error sqrt(var / n) (float bits; values >= 0
+// order like their bit patterns), written with one atomic per warp.
+__global__ void max_stderr_kernel(const double* __restrict__ sum, const double* __restrict__ sum_sq,
+                                  const uint32_t* __restrict__ count, int64_t n, unsigned* __restrict__ out) {
+  float m = 0.0f;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double c = count[i];
+    float se = INFINITY;
+    if (c >= 2.0) {
+      const double mean = sum[i] / c;
+      const double var = fmax(0.0, (sum_sq[i] - c * mean * mean) / (c - 1.0));
+      se = static_cast<float>(sqrt(var / c));
+    }
+    m = fmaxf(m, se);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// First-fit allocator over offsets of one device pool (256-byte granules).
+class PoolAllocator {
+ public:
+  explicit PoolAllocator(size_t bytes) : capacity_(bytes) { free_[0] = bytes; }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) & ~size_t{255};
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes, start = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[start] = rest;
+        used_ += bytes;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 255) & ~size_t{255};
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t capacity() const { return capacity_; }
+  size_t used() const { return used_; }
+
+ private:
+  size_t capacity_;
+  size_t used_ = 0;
+  std::map<size_t, size_t> free_;
+};
+
+// Device bytes a request of n points holds while in flight: points (12 B) and
+// accumulators (sum, sum_sq, steps: 8 B; count, forced: 4 B).
+size_t request_bytes(int64_t n) { return static_cast<size_t>(n) * 44 + 5 * 256; }
+
+}  // namespace
+}  // namespace n2w
+
+using namespace n2w;
+
+struct n2w_server {
+  struct Request {
+    int64_t id = 0;
+    n2w_request req{};
+    std::vector<float> h_points;
+    int state = N2W_REQUEST_PENDING;
+    std::string error;
+    // device residency
+    size_t pool_off = 0, pool_len = 0;
+    n2w_vec3* d_points = nullptr;
+    double *sum = nullptr, *sum_sq = nullptr;
+    uint64_t* steps = nullptr;
+    uint32_t *count = nullptr, *forced = nullptr;
+    // progress
+    int64_t cursor = 0;         // next point of the current sweep
+    int sweep = 0;              // index of the current sweep
+    int sweep_walks = 0;        // walks per point of the current sweep
+    int64_t walks_done = 0;     // walks per point completed
+    float max_stderr = INFINITY;
+    int ticks = 0;
+    // results
+    std::vector<double> mean, stderr_;
+    int64_t t_submit = 0, t_admit = 0, t_finish = 0;
+  };
+
+  std::unique_ptr<n2w_scene> scene;
+  std::vector<n2w_problem> problems;
+  n2w_problem* d_problems = nullptr;
+  n2w_server_options opt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  char* d_pool = nullptr;
+  std::unique_ptr<PoolAllocator> pool;
+  BatchInst* d_insts = nullptr;
+  BatchInst* h_insts = nullptr;  // pinned staging of the tick's instance table
+  float4* d_cpd = nullptr;
+  int2* d_ids = nullptr;
+  int64_t tick_point_cap = 0;
+  char* d_hdr = nullptr;         // queue counter + run counters of a tick
+  unsigned* d_conv = nullptr;    // per-slot max stderr (float bits)
+  unsigned* h_conv = nullptr;    // pinned
+  n2w_walk_counters* h_counters = nullptr;  // pinned
+
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<int64_t> pending;
+  std::vector<int64_t> active;
+  std::unordered_map<int64_t, std::unique_ptr<Request>> requests;
+  int64_t next_id = 1;
+  bool stop = false;
+  std::string fatal;
+  std::thread worker;
+  n2w_server_stats stats{};
+};
+
+namespace {
+
+void fail_all_locked(n2w_server& s, const std::string& msg) {
+  s.fatal = msg;
+  for (auto& kv : s.requests) {
+    auto& r = *kv.second;
+    if (r.state == N2W_REQUEST_PENDING || r.state == N2W_REQUEST_ACTIVE) {
+      r.state = N2W_REQUEST_FAILED;
+      r.error = msg;
+      r.t_finish = now_ns();
+    }
+  }
+  s.pending.clear();
+  s.active.clear();
+  s.cv_done.notify_all();
+}
+
+// Admits pending requests in arrival order while the pool and the in-flight
+// limit allow; uploads points and zeroes accumulators.  Called without the lock.
+void admit(n2w_server& s) {
+  std::vector<n2w_server::Request*> admitted;
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    while (!s.pending.empty() && static_cast<int>(s.active.size()) < s.opt.max_inflight) {
+      auto& r = *s.requests.at(s.pending.front());
+      const int64_t n = r.req.point_count;
+      size_t off = 0;
+      if (!s.pool->alloc(request_bytes(n), &off)) break;  // head-of-line waits for memory
+      s.pending.pop_front();
+      r.pool_off = off;
+      r.pool_len = request_bytes(n);
+      char* base = s.d_pool + off;
+      auto carve = [&](size_t bytes) {
+        char* p = base;
+        base += (bytes + 255) & ~size_t{255};
+        return p;
+      };
+      r.sum = reinterpret_cast<double*>(carve(8 * n));
+      r.sum_sq = reinterpret_cast<double*>(carve(8 * n));
+      r.steps = reinterpret_cast<uint64_t*>(carve(8 * n));
+      r.count = reinterpret_cast<uint32_t*>(carve(4 * n));
+      r.forced = reinterpret_cast<uint32_t*>(carve(4 * n));
+      r.d_points = reinterpret_cast<n2w_vec3*>(carve(12 * n));
+      r.state = N2W_REQUEST_ACTIVE;
+      r.t_admit = now_ns();
+      r.sweep_walks = std::min(r.req.max_walks_per_point, std::max(32, r.req.min_walks_per_point));
+      s.active.push_back(r.id);
+      admitted.push_back(&r);
+      s.stats.peak_inflight = std::max<int64_t>(s.stats.peak_inflight, static_cast<int64_t>(s.active.size()));
+      s.stats.peak_pool_bytes = std::max<int64_t>(s.stats.peak_pool_bytes, static_cast<int64_t>(s.pool->used()));
+    }
+  }
+  for (auto* r : admitted) {
+    const int64_t n = r->req.point_count;
+    N2W_CUDA(cudaMemsetAsync(r->sum, 0, 8 * n, s.stream));
+    N2W_CUDA(cudaMemsetAsync(r->sum_sq, 0, 8 * n, s.stream));
+    N2W_CUDA(cudaMemsetAsync(r->steps, 0, 8 * n, s.stream));
+    N2W_CUDA(cudaMemsetAsync(r->count, 0, 4 * n, s.stream));
+    N2W_CUDA(cudaMemsetAsync(r->forced, 0, 4 * n, s.stream));
+    N2W_CUDA(cudaMemcpyAsync(r->d_points, r->h_points.data(), 12 * n, cudaMemcpyHostToDevice, s.stream));
+  }
+}
+
+struct Slice {
+  n2w_server::Request* r;
+  int64_t first, count;  // point range of this tick
+};
+
+// One tick: share the walk budget, launch the batched walker over every
+// active request's next point range, advance cursors, check finished sweeps.
+void tick(n2w_server& s) {
+  std::vector<n2w_server::Request*> act;
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    for (int64_t id : s.active) act.push_back(s.requests.at(id).get());
+  }
+  if (act.empty()) return;
+  // Water-filling of the tick's walk budget over the requests' remaining sweep work.
+  const int64_t budget = s.opt.tick_walks;
+  std::vector<int64_t> want(act.size()), give(act.size(), 0);
+  for (size_t k = 0; k < act.size(); ++k) {
+    want[k] = (act[k]->req.point_count - act[k]->cursor) * static_cast<int64_t>(act[k]->sweep_walks);
+  }
+  int64_t left = budget;
+  std::vector<size_t> open;
+  for (size_t k = 0; k < act.size(); ++k) open.push_back(k);
+  while (!open.empty() && left > 0) {
+    const int64_t share = std::max<int64_t>(1, left / static_cast<int64_t>(open.size()));
+    std::vector<size_t> still;
+    int64_t used = 0;
+    for (size_t k : open) {
+      const int64_t g = std::min(want[k] - give[k], share);
+      give[k] += g;
+      used += g;
+      if (give[k] < want[k]) still.push_back(k);
+    }
+    left -= used;
+    if (still.size() == open.size() && used == 0) break;
+    open.swap(still);
+  }
+  std::vector<Slice> slices;
+  int64_t tick_points = 0;
+  for (size_t k = 0; k < act.size(); ++k) {
+    auto* r = act[k];
+    int64_t pts = give[k] / r->sweep_walks;
+    pts = std::max<int64_t>(pts, 1);  // every request advances every tick
+    pts = std::min(pts, r->req.point_count - r->cursor);
+    pts = std::min(pts, s.tick_point_cap - tick_points);
+    if (pts <= 0) continue;
+    slices.push_back({r, r->cursor, pts});
+    tick_points += pts;
+  }
+  if (slices.empty()) return;
+  const int chunk = kDefaultChunk;
+  int64_t cbase = 0, pbase = 0;
+  for (size_t i = 0; i < slices.size(); ++i) {
+    const Slice& sl = slices[i];
+    auto* r = sl.r;
+    BatchInst& I = s.h_insts[i];
+    I = BatchInst{};
+    I.points = r->d_points + sl.first;
+    I.sum = r->sum + sl.first;
+    I.sum_sq = r->sum_sq + sl.first;
+    I.count = r->count + sl.first;
+    I.steps = r->steps + sl.first;
+    I.forced = r->forced + sl.first;
+    I.point_base = pbase;
+    I.point_count = sl.count;
+    I.chunk_base = cbase;
+    I.walks_per_point = r->sweep_walks;
+    I.chunks_per_point = (r->sweep_walks + chunk - 1) / chunk;
+    set_instance_geometry(I, *s.scene, r->req.mesh);
+    set_instance_problem(I, s.problems[r->req.problem], s.d_problems + r->req.problem);
+    // sweep key; walk ids p * W + w over the whole request (p = global point index)
+    philox_key(r->req.seed + 0x9E3779B97F4A7C15ull * static_cast<uint64_t>(r->sweep + 1), 0u, I.k0, I.k1);
+    I.wid_base = sl.first * static_cast<int64_t>(r->sweep_walks);
+    pbase += sl.count;
+    cbase += sl.count * I.chunks_per_point;
+  }
+  const cudaStream_t st = s.stream;
+  N2W_CUDA(cudaMemcpyAsync(s.d_insts, s.h_insts, sizeof(BatchInst) * slices.size(), cudaMemcpyHostToDevice, st));
+  N2W_CUDA(cudaMemsetAsync(s.d_hdr, 0, 512, st));
+  WalkArgs a{};
+  a.nodes = reinterpret_cast<const float4*>(s.scene->d_nodes);
+  a.tris = reinterpret_cast<const float4*>(s.scene->d_tris);
+  a.first_cpd = s.d_cpd;
+  a.first_ids = s.d_ids;
+  a.total_chunks = cbase;
+  a.chunk = chunk;
+  a.regen = s.opt.regen_threshold > 0 ? s.opt.regen_threshold : kDefaultRegen;
+  a.max_steps = s.opt.max_steps;
+  a.eps = s.opt.epsilon;
+  a.step_scale = s.opt.step_scale;
+  a.queue = reinterpret_cast<unsigned long long*>(s.d_hdr);
+  a.counters = reinterpret_cast<n2w_walk_counters*>(s.d_hdr + 256);
+  a.insts = s.d_insts;
+  a.n_insts = static_cast<int>(slices.size());
+  launch_first_query_batch(a, pbase, s.d_cpd, s.d_ids, st);
+  launch_walker_batch(a, s.opt.block_size > 0 ? s.opt.block_size : kDefaultWalkerThreads, 0, 0, st);
+  N2W_CUDA(cudaMemcpyAsync(s.h_counters, s.d_hdr + 256, sizeof(n2w_walk_counters), cudaMemcpyDeviceToHost, st));
+  // Requests whose sweep ends with this tick: reduce their max stderr.
+  std::vector<n2w_server::Request*> swept;
+  for (const Slice& sl : slices) {
+    if (sl.first + sl.count == sl.r->req.point_count) swept.push_back(sl.r);
+  }
+  if (!swept.empty()) {
+    N2W_CUDA(cudaMemsetAsync(s.d_conv, 0, sizeof(unsigned) * swept.size(), st));
+    for (size_t i = 0; i < swept.size(); ++i) {
+      const int64_t n = swept[i]->req.point_count;
+      const int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 1024));
+      max_stderr_kernel<<<grid, 256, 0, st>>>(swept[i]->sum, swept[i]->sum_sq, swept[i]->count, n, s.d_conv + i);
+      N2W_CUDA(cudaGetLastError());
+    }
+    N2W_CUDA(cudaMemcpyAsync(s.h_conv, s.d_conv, sizeof(unsigned) * swept.size(), cudaMemcpyDeviceToHost, st));
+  }
+  N2W_CUDA(cudaStreamSynchronize(st));
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.stats.ticks += 1;
+    s.stats.walks += static_cast<int64_t>(s.h_counters->walks);
+    s.stats.walk_steps += static_cast<int64_t>(s.h_counters->steps);
+    s.stats.overflow += static_cast<int64_t>(s.h_counters->overflow);
+  }
+  for (const Slice& sl : slices) {
+    sl.r->cursor += sl.count;
+    sl.r->ticks += 1;
+  }
+  // Sweep bookkeeping and completion.
+  for (size_t i = 0; i < swept.size(); ++i) {
+    auto* r = swept[i];
+    float se;
+    std::memcpy(&se, &s.h_conv[i], sizeof(float));
+    r->max_stderr = se;
+    r->walks_done += r->sweep_walks;
+    r->cursor = 0;
+    r->sweep += 1;
+    const bool reached = se <= r->req.target_stderr && r->walks_done >= r->req.min_walks_per_point;
+    const bool capped = r->walks_done >= r->req.max_walks_per_point;
+    if (reached || capped) {
+      const int64_t n = r->req.point_count;
+      std::vector<double> sum(n), sum_sq(n);
+      std::vector<uint32_t> cnt(n);
+      N2W_CUDA(cudaMemcpyAsync(sum.data(), r->sum, 8 * n, cudaMemcpyDeviceToHost, st));
+      N2W_CUDA(cudaMemcpyAsync(sum_sq.data(), r->sum_sq, 8 * n, cudaMemcpyDeviceToHost, st));
+      N2W_CUDA(cudaMemcpyAsync(cnt.data(), r->count, 4 * n, cudaMemcpyDeviceToHost, st));
+      N2W_CUDA(cudaStreamSynchronize(st));
+      r->mean.resize(n);
+      r->stderr_.resize(n);
+      for (int64_t p = 0; p < n; ++p) {
+        const double c = cnt[p];
+        const double m = c > 0 ? sum[p] / c : 0.0;
+        const double v = c > 1 ? std::max(0.0, (sum_sq[p] - c * m * m) / (c - 1.0)) : 0.0;
+        r->mean[p] = m;
+        r->stderr_[p] = c > 0 ? std::sqrt(v / c) : INFINITY;
+      }
+      std::lock_guard<std::mutex> lk(s.mu);
+      s.pool->release(r->pool_off, r->pool_len);
+      r->state = reached ? N2W_REQUEST_DONE : N2W_REQUEST_CAPPED;
+      r->t_finish = now_ns();
+      r->h_points.clear();
+      r->h_points.shrink_to_fit();
+      s.active.erase(std::find(s.active.begin(), s.active.end(), r->id));
+      s.stats.completed += 1;
+      s.cv_done.notify_all();
+    } else {
+      // Next sweep: the walks the standard-error model predicts are still
+      // needed (stderr ~ 1/sqrt(N)), plus 10 %, within [32, cap - done].
+      const double need = static_cast<double>(r->walks_done) *
+                              std::pow(static_cast<double>(se) / r->req.target_stderr, 2.0) * 1.1 -
+                          static_cast<double>(r->walks_done);
+      int64_t w = static_cast<int64_t>(std::ceil(std::isfinite(need) ? need : 1e9));
+      w = std::max<int64_t>(w, std::max<int64_t>(32, r->req.min_walks_per_point - r->walks_done));
+      w = std::min<int64_t>(w, r->req.max_walks_per_point - r->walks_done);
+      w = std::min<int64_t>(w, 1 << 20);
+      r->sweep_walks = static_cast<int>(std::max<int64_t>(w, 1));
+    }
+  }
+}
+
+void worker_loop(n2w_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty() || !s->active.empty(); });
+      if (s->stop) return;
+    }
+    try {
+      admit(*s);
+      tick(*s);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      fail_all_locked(*s, std::string("serving loop stopped: ") + e.what());
+      return;
+    }
+  }
+}
+
+void destroy_server(n2w_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (auto& kv : s->requests) {
+      auto& r = *kv.second;
+      if (r.state == N2W_REQUEST_PENDING || r.state == N2W_REQUEST_ACTIVE) {
+        r.state = N2W_REQUEST_FAILED;
+        r.error = "server destroyed";
+      }
+    }
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  cudaFree(s->d_pool);
+  cudaFree(s->d_insts);
+  cudaFree(s->d_cpd);
+  cudaFree(s->d_ids);
+  cudaFree(s->d_hdr);
+  cudaFree(s->d_conv);
+  cudaFree(s->d_problems);
+  cudaFreeHost(s->h_insts);
+  cudaFreeHost(s->h_conv);
+  cudaFreeHost(s->h_counters);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->scene) {
+    n2w_scene_destroy(s->scene.release());
+  }
+  delete s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int n2w_server_options_default(n2w_server_options* out) {
+  return guarded([&] {
+    N2W_REQUIRE(out, "null output");
+    *out = n2w_server_options{};
+    out->pool_bytes = 0;
+    out->pool_fraction = 0.25f;
+    out->max_inflight = 256;
+    out->tick_walks = 1 << 21;
+    out->max_steps = 256;
+    out->epsilon = 1.0e-3f;
+    out->step_scale = 0.999f;
+    out->block_size = 256;
+    out->regen_threshold = 8;
+  });
+}
+
+int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_problem* problems, int problem_count,
+                      const n2w_server_options* options, n2w_server** out) {
+  n2w_server* s = nullptr;
+  const int st = guarded([&] {
+    N2W_REQUIRE(bvhs && problems && out && mesh_count > 0 && problem_count > 0, "n2w_server_create: bad arguments");
+    n2w_server_options o{};
+    if (options) o = *options;
+    else n2w_server_options_default(&o);
+    N2W_REQUIRE(o.max_inflight >= 1 && o.max_inflight <= 65536, "max_inflight must be in [1, 65536]");
+    N2W_REQUIRE(o.tick_walks >= 1024, "tick_walks must be >= 1024");
+    N2W_REQUIRE(o.max_steps > 0 && o.epsilon > 0.0f && o.step_scale > 0.0f && o.step_scale <= 1.0f,
+                "invalid walk options");
+    N2W_REQUIRE(o.block_size == 0 || (o.block_size >= 32 && o.block_size <= kWalkerMaxThreads && o.block_size % 32 == 0),
+                "block_size must be 0 or a multiple of 32 in [32, 256]");
+    for (int p = 0; p < problem_count; ++p) validate_problem(problems[p]);
+    s = new n2w_server();
+    s->opt = o;
+    N2W_CUDA(cudaGetDevice(&s->device));
+    n2w_scene* sc = nullptr;
+    const int rc = n2w_scene_create(bvhs, mesh_count, &sc);
+    if (rc != N2W_OK) throw Error(rc, n2w_last_error());
+    s->scene.reset(sc);
+    s->problems.assign(problems, problems + problem_count);
+    N2W_CUDA(cudaMalloc(&s->d_problems, sizeof(n2w_problem) * problem_count));
+    N2W_CUDA(cudaMemcpy(s->d_problems, problems, sizeof(n2w_problem) * problem_count, cudaMemcpyHostToDevice));
+    size_t pool = static_cast<size_t>(o.pool_bytes);
+    if (pool == 0) {
+      size_t fr = 0, tot = 0;
+      N2W_CUDA(cudaMemGetInfo(&fr, &tot));
+      const float f = o.pool_fraction > 0.0f && o.pool_fraction <= 0.9f ? o.pool_fraction : 0.25f;
+      pool = static_cast<size_t>(static_cast<double>(fr) * f);
+    }
+    pool &= ~size_t{255};
+    N2W_REQUIRE(pool >= (1u << 20), "device pool below 1 MiB");
+    N2W_CUDA(cudaMalloc(&s->d_pool, pool));
+    s->pool = std::make_unique<PoolAllocator>(pool);
+    s->opt.pool_bytes = static_cast<int64_t>(pool);
+    // A tick holds at most one instance per in-flight request and at most
+    // tick_walks / 32 + max_inflight points (sweeps have >= 32 walks per point).
+    s->tick_point_cap = o.tick_walks / 32 + o.max_inflight;
+    N2W_CUDA(cudaMalloc(&s->d_insts, sizeof(BatchInst) * o.max_inflight));
+    N2W_CUDA(cudaMallocHost(&s->h_insts, sizeof(BatchInst) * o.max_inflight));
+    N2W_CUDA(cudaMalloc(&s->d_cpd, sizeof(float4) * s->tick_point_cap));
+    N2W_CUDA(cudaMalloc(&s->d_ids, sizeof(int2) * s->tick_point_cap));
+    N2W_CUDA(cudaMalloc(&s->d_hdr, 512));
+    N2W_CUDA(cudaMalloc(&s->d_conv, sizeof(unsigned) * o.max_inflight));
+    N2W_CUDA(cudaMallocHost(&s->h_conv, sizeof(unsigned) * o.max_inflight));
+    N2W_CUDA(cudaMallocHost(&s->h_counters, sizeof(n2w_walk_counters)));
+    N2W_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->worker = std::thread(worker_loop, s);
+    *out = s;
+  });
+  if (st != N2W_OK && s) destroy_server(s);
+  return st;
+}
+
+int n2w_server_submit(n2w_server* s, const n2w_request* req, const float* h_points, int64_t* id_out) {
+  return guarded([&] {
+    N2W_REQUIRE(s && req && id_out, "n2w_server_submit: null argument");
+    N2W_REQUIRE(req->mesh >= 0 && req->mesh < static_cast<int>(s->scene->meshes.size()), "mesh index out of range");
+    N2W_REQUIRE(req->problem >= 0 && req->problem < static_cast<int>(s->problems.size()),
+                "problem index out of range");
+    N2W_REQUIRE(req->point_count > 0 && h_points, "a request needs at least one point");
+    N2W_REQUIRE(req->target_stderr > 0.0f, "target_stderr must be positive");
+    N2W_REQUIRE(req->max_walks_per_point >= 1 && req->min_walks_per_point >= 0 &&
+                    req->min_walks_per_point <= req->max_walks_per_point,
+                "need 0 <= min_walks_per_point <= max_walks_per_point, max >= 1");
+    if (request_bytes(req->point_count) > s->pool->capacity()) {
+      throw Error(N2W_ENOMEM, "request of " + std::to_string(req->point_count) +
+                                  " points needs more device memory than the whole serving pool (" +
+                                  std::to_string(s->pool->capacity()) + " bytes)");
+    }
+    auto r = std::make_unique<n2w_server::Request>();
+    r->req = *req;
+    r->h_points.assign(h_points, h_points + 3 * req->point_count);
+    r->t_submit = now_ns();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->fatal.empty()) throw Error(N2W_ECUDA, s->fatal);
+    r->id = s->next_id++;
+    *id_out = r->id;
+    s->pending.push_back(r->id);
+    s->requests.emplace(r->id, std::move(r));
+    s->stats.submitted += 1;
+    s->cv_work.notify_one();
+  });
+}
+
+int n2w_server_poll(n2w_server* s, int64_t id, int* state_out) {
+  return guarded([&] {
+    N2W_REQUIRE(s && state_out, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    N2W_REQUIRE(it != s->requests.end(), "unknown request id");
+    *state_out = it->second->state;
+  });
+}
+
+int n2w_server_wait(n2w_server* s, int64_t id, double timeout_seconds, double* h_mean, double* h_stderr,
+                    n2w_request_info* info) {
+  return guarded([&] {
+    N2W_REQUIRE(s, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    N2W_REQUIRE(it != s->requests.end(), "unknown request id (or already collected)");
+    n2w_server::Request* r = it->second.get();
+    auto finished = [&] {
+      return r->state == N2W_REQUEST_DONE || r->state == N2W_REQUEST_CAPPED || r->state == N2W_REQUEST_FAILED;
+    };
+    if (timeout_seconds < 0) {
+      s->cv_done.wait(lk, finished);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_seconds), finished)) {
+      throw Error(N2W_ETIMEOUT, "request " + std::to_string(id) + " still running");
+    }
+    if (info) {
+      *info = n2w_request_info{};
+      info->state = r->state;
+      info->walks_per_point = r->walks_done;
+      info->sweeps = r->sweep;
+      info->ticks = r->ticks;
+      info->max_stderr = r->max_stderr;
+      info->queue_seconds = (r->t_admit ? r->t_admit - r->t_submit : 0) * 1e-9;
+      info->latency_seconds = (r->t_finish - r->t_submit) * 1e-9;
+    }
+    if (r->state == N2W_REQUEST_FAILED) {
+      const std::string msg = r->error;
+      s->requests.erase(it);
+      throw Error(N2W_ECUDA, msg);
+    }
+    const int64_t n = r->req.point_count;
+    if (h_mean) std::memcpy(h_mean, r->mean.data(), 8 * n);
+    if (h_stderr) std::memcpy(h_stderr, r->stderr_.data(), 8 * n);
+    s->requests.erase(it);
+  });
+}
+
+int n2w_server_get_stats(n2w_server* s, n2w_server_stats* out) {
+  return guarded([&] {
+    N2W_REQUIRE(s && out, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
+    out->inflight = static_cast<int64_t>(s->active.size());
+    out->pending = static_cast<int64_t>(s->pending.size());
+    out->pool_bytes = static_cast<int64_t>(s->pool->capacity());
+    out->pool_used = static_cast<int64_t>(s->pool->used());
+  });
+}
+
+void n2w_server_destroy(n2w_server* s) { destroy_server(s); }
+
+}  // extern "C"

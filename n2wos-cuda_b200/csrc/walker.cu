@@ -463,11 +463,13 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
             wpp = I.walks_per_point;
             walk = static_cast<int>((lc % cpp) * a.chunk);
             pid = I.point_base + lpid;
+            wid = static_cast<uint64_t>(I.wid_base);
           } else {
             lpid = static_cast<int64_t>(c / static_cast<unsigned long long>(a.chunks_per_point));
             wpp = a.walks_per_point;
             walk = static_cast<int>((c % static_cast<unsigned long long>(a.chunks_per_point)) * a.chunk);
             pid = lpid;
+            wid = 0;
           }
           walk_end = min(walk + a.chunk, wpp);
           const n2w_vec3 p0 = start_point();
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
           cont0 = 0;
           has_xm = false;
           w_overflow = false;
-          wid = static_cast<uint64_t>(lpid) * static_cast<uint64_t>(wpp) + static_cast<uint64_t>(walk);
+          wid += static_cast<uint64_t>(lpid) * static_cast<uint64_t>(wpp) + static_cast<uint64_t>(walk);
           const float4 cc = __ldg(a.first_cpd + pid);
           const int2 ii = __ldg(a.first_ids + pid);
           hit.cp = dev::v3(cc.x, cc.y, cc.z);

@@ -41,6 +41,7 @@ struct alignas(16) BatchInst {
   int32_t root;                 // root node of this instance's mesh in the scene
   uint32_t k0, k1;              // Philox key of the instance
   int32_t has_source, source_center, source_samples, pad;
+  int64_t wid_base;             // added to every walk id (a point range of a larger request)
 };
 
 struct WalkArgs {

@@ -20,7 +20,7 @@ __all__ = [
     "problem_sinprod", "problem_reference", "problem_from_name", "walk_options", "wos_estimate",
     "N2wError", "LIB_PATH", "EXPORTED", "N2W_BC", "device_count", "device_summary", "runtime_version",
     "N2W_SOURCE_BALL", "N2W_SOURCE_CENTER", "N2W_WALK_PURE", "N2W_WALK_PREFIX", "N2W_WALK_RESIDUAL",
-    "Scene", "Batch",
+    "Scene", "Batch", "Server",
 ]
 
 
@@ -568,6 +568,69 @@ class Batch:
         if getattr(self, "_h", None):
             lib.n2w_batch_destroy(self._h)
             self._h = None
+
+
+class Server:
+    """Continuous-batching WoS server (native worker thread; see n2w_server_*).
+
+    meshes: list of Bvh; problems: list of Problem.  submit() returns a request
+    id; wait() returns (mean, stderr, info dict)."""
+
+    def __init__(self, bvhs, problems, **options):
+        from ._lib import ServerOptions
+
+        o = ServerOptions()
+        call("n2w_server_options_default", C.byref(o))
+        for k, v in options.items():
+            setattr(o, k, v)
+        self.options = o
+        arr = (C.c_void_p * len(bvhs))(*[b.handle for b in bvhs])
+        self._problems = (Problem * len(problems))(*problems)
+        h = C.c_void_p()
+        call("n2w_server_create", arr, len(bvhs), self._problems, len(problems), C.byref(o), C.byref(h))
+        self._h = h
+        self._sizes = {}
+
+    def submit(self, mesh: int, problem: int, points: np.ndarray, target_stderr: float, seed: int = 1,
+               min_walks: int = 32, max_walks: int = 1 << 16) -> int:
+        from ._lib import Request
+
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        r = Request(mesh, problem, len(pts), target_stderr, min_walks, max_walks, seed)
+        rid = C.c_int64()
+        call("n2w_server_submit", self._h, C.byref(r), _ptr(pts), C.byref(rid))
+        self._sizes[rid.value] = len(pts)
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        st = C.c_int()
+        call("n2w_server_poll", self._h, rid, C.byref(st))
+        return st.value
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        from ._lib import RequestInfo
+
+        n = self._sizes.pop(rid)
+        mean = np.empty(n, np.float64)
+        se = np.empty(n, np.float64)
+        info = RequestInfo()
+        call("n2w_server_wait", self._h, rid, C.c_double(timeout), _ptr(mean), _ptr(se), C.byref(info))
+        return mean, se, {f: getattr(info, f) for f, _ in RequestInfo._fields_}
+
+    def stats(self) -> dict:
+        from ._lib import ServerStats
+
+        s = ServerStats()
+        call("n2w_server_get_stats", self._h, C.byref(s))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.n2w_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def cache_config(**overrides):

@@ -120,6 +120,30 @@ class BatchTuning(C.Structure):
                 ("regen_threshold", C.c_int32), ("reg_variant", C.c_int32), ("ms", C.c_float)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("pool_bytes", C.c_int64), ("pool_fraction", C.c_float), ("max_inflight", C.c_int32),
+                ("tick_walks", C.c_int64), ("max_steps", C.c_int32), ("epsilon", C.c_float),
+                ("step_scale", C.c_float), ("block_size", C.c_int32), ("regen_threshold", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("mesh", C.c_int32), ("problem", C.c_int32), ("point_count", C.c_int64),
+                ("target_stderr", C.c_float), ("min_walks_per_point", C.c_int32),
+                ("max_walks_per_point", C.c_int32), ("seed", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("sweeps", C.c_int32), ("walks_per_point", C.c_int64), ("ticks", C.c_int64),
+                ("max_stderr", C.c_float), ("queue_seconds", C.c_double), ("latency_seconds", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in
+                ("submitted", "completed", "inflight", "pending", "peak_inflight", "ticks", "walks", "walk_steps",
+                 "overflow", "pool_bytes", "pool_used", "peak_pool_bytes")]
+
+
+N2W_REQUEST_PENDING, N2W_REQUEST_ACTIVE, N2W_REQUEST_DONE, N2W_REQUEST_CAPPED, N2W_REQUEST_FAILED = range(5)
 N2W_LABEL_EXACT, N2W_LABEL_WOS = 0, 1
 N2W_SLICE_RULE_RENDER, N2W_SLICE_RULE_EVAL = 0, 1
 
@@ -218,6 +242,13 @@ _SIGS = {
     "n2w_batch_autotune": (I, [P, C.c_double, C.POINTER(BatchTuning), C.POINTER(BatchTuning), I, C.POINTER(I), P]),
     "n2w_batch_set_tuning": (I, [P, C.POINTER(BatchTuning), P]),
     "n2w_batch_destroy": (None, [P]),
+    "n2w_server_options_default": (I, [C.POINTER(ServerOptions)]),
+    "n2w_server_create": (I, [C.POINTER(C.c_void_p), I, C.POINTER(Problem), I, C.POINTER(ServerOptions), PP]),
+    "n2w_server_submit": (I, [P, C.POINTER(Request), P, C.POINTER(I64)]),
+    "n2w_server_poll": (I, [P, I64, C.POINTER(I)]),
+    "n2w_server_wait": (I, [P, I64, C.c_double, P, P, C.POINTER(RequestInfo)]),
+    "n2w_server_get_stats": (I, [P, C.POINTER(ServerStats)]),
+    "n2w_server_destroy": (None, [P]),
     "n2w_device_count": (I, [C.POINTER(I)]),
     "n2w_set_device": (I, [I]),
     "n2w_malloc": (I, [PP, C.c_size_t]),
