@@ -424,6 +424,144 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Serving loop under mixed load: Poisson arrivals of requests on 4
+    device-resident meshes (the config-0 bumpy sphere, the config-1 icosphere,
+    the smallest and largest config-3 spheres) with either an 8-charge harmonic
+    boundary or the config-1 manufactured Poisson problem; points uniform in
+    the interior (ball r = 0.9 masked by the mesh); a fraction of large
+    requests.  Each request stops when the root mean square of its per-point
+    standard errors meets its target.  Latency is measured natively
+    (submission -> result ready).  The run stops at --serve-time-limit and
+    then reports how many requests had not finished."""
+    import threading as th
+
+    import n2w
+    from n2w import workloads
+    from n2w._lib import N2W_ETIMEOUT, call
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    call("n2w_set_device", local)
+    rng = np.random.default_rng(args.serve_seed)
+    meshes = [workloads.bumpy_sphere(n2w, 128, 256), n2w.Mesh.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345),
+              workloads.bumpy_sphere(n2w, 32, 64), workloads.bumpy_sphere(n2w, 256, 512)]
+    meshes[1].normalize()
+    bvhs = [n2w.Bvh(m, 4, "sah") for m in meshes]
+    pool_pts = [workloads.interior_ball_points(b, 65536, rng) for b in bvhs]
+    problems = [n2w.problem_charges_seeded(8, 1.6, 2.0, seed=2024), n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)]
+    problems[1].source_samples = args.serve_source_samples  # variance reduction of the Poisson source term
+    srv = n2w.Server(bvhs, problems, tick_walks=args.serve_tick_walks, epsilon=1e-3)
+    N = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, N))
+    reqs = []
+    for k in range(N):
+        large = rng.uniform() < args.serve_large_fraction
+        lo, hi = (4096, args.serve_large_max) if large else (1, 4096)
+        n = min(workloads.log_uniform_int(rng, lo, hi), 65536)
+        mesh = int(rng.integers(0, 4))
+        prob = int(rng.uniform() < args.serve_poisson_fraction)
+        tgt = 1e-3 if (prob == 0 and n <= 256 and rng.uniform() < 0.5) else 1e-2
+        off = int(rng.integers(0, 65536 - n + 1))
+        reqs.append({"t": float(arrivals[k]), "n": n, "mesh": mesh, "problem": prob, "target": tgt, "off": off,
+                     "seed": int(rng.integers(1, 2**62))})
+    ids = [None] * N
+    stop = th.Event()
+    errors = []
+    t0 = time.perf_counter()
+
+    def submitter():
+        try:
+            for k, r in enumerate(reqs):
+                while not stop.is_set():
+                    dt = r["t"] - (time.perf_counter() - t0)
+                    if dt <= 0:
+                        break
+                    time.sleep(min(dt, 0.05))
+                if stop.is_set():
+                    return
+                pts = pool_pts[r["mesh"]][r["off"]:r["off"] + r["n"]]
+                ids[k] = srv.submit(r["mesh"], r["problem"], pts, r["target"], seed=r["seed"],
+                                    max_walks=args.serve_max_walks, rms=True)
+        except Exception as e:  # surfaced by the collector below
+            errors.append(e)
+            stop.set()
+
+    sub = th.Thread(target=submitter, daemon=True)
+    deadline = t0 + args.serve_time_limit
+    results = []
+    last = t0
+    with ClockSampler(local) as clocks:
+        sub.start()
+        k = 0
+        while k < N and not errors:
+            now = time.perf_counter()
+            if now > deadline:
+                break
+            if now - last > 5.0:
+                st = srv.stats()
+                print(f"[serve] t={now - t0:.0f}s done={k}/{N} submitted={st['submitted']} "
+                      f"inflight={st['inflight']} pending={st['pending']} ticks={st['ticks']} "
+                      f"walk_steps={st['walk_steps']:.3g}", file=sys.stderr, flush=True)
+                last = now
+            if ids[k] is None:
+                time.sleep(0.001)
+                continue
+            try:
+                mean, se, info = srv.wait(ids[k], timeout=min(1.0, max(0.01, deadline - now)))
+            except n2w.N2wError as e:
+                if e.code == N2W_ETIMEOUT:
+                    continue
+                raise
+            r = reqs[k]
+            pts = pool_pts[r["mesh"]][r["off"]:r["off"] + r["n"]]
+            exact = n2w.problem_exact(problems[r["problem"]], pts.astype(np.float64))
+            results.append({"n": r["n"], "latency": info["latency_seconds"], "queue": info["queue_seconds"],
+                            "mse": float(np.mean((mean - exact) ** 2)), "target": r["target"],
+                            "state": info["state"], "walks": info["walks_per_point"]})
+            k += 1
+        stop.set()
+        makespan = time.perf_counter() - t0
+    if errors:
+        raise errors[0]
+    st = srv.stats()
+    srv.close()
+    sub.join(timeout=5)
+    done = len(results)
+    lat = np.array([r["latency"] for r in results]) if results else np.array([np.nan])
+    small = np.array([r["latency"] for r in results if r["n"] <= 4096]) if results else np.array([np.nan])
+    mse_ratio = np.array([r["mse"] / r["target"] ** 2 for r in results]) if results else np.array([np.nan])
+    complete = done == N
+    line = {
+        "metric": "p99 latency of <=4096-point requests, serving loop under mixed load (s)",
+        "value": float(np.percentile(small, 99)) if complete else None, "unit": "s", "n_gpus": 1, "steps": N,
+        "warmup": 0, "ms_per_step": 1e3 * makespan / max(done, 1), "higher_is_better": False, "scaling": "none",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{N} requests, Poisson arrivals at {args.serve_rate}/s, 4 meshes (bumpy sphere "
+                               "128x256, icosphere L6, bumpy spheres 32x64 and 256x512), problems: 8-charge "
+                               f"harmonic / sin-product Poisson ({100 * args.serve_poisson_fraction:.0f}%, "
+                               f"{args.serve_source_samples} source samples per ball), points "
+                               f"log-uniform 1..4096 ({100 * args.serve_large_fraction:.0f}% log-uniform "
+                               f"4096..{args.serve_large_max}), RMS stderr target 1e-2 (1e-3 for half of the "
+                               "<=256-point harmonic requests)",
+                   "tick_walks": args.serve_tick_walks, "max_walks_per_point": args.serve_max_walks,
+                   "seed": args.serve_seed, "time_limit_s": args.serve_time_limit},
+        "complete": complete, "finished_requests": done,
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "p50_le4096": float(np.percentile(small, 50)), "p99_le4096": float(np.percentile(small, 99)),
+                      "max": float(np.max(lat))},
+        "throughput": {"requests_per_s": done / makespan, "points_per_s": sum(r["n"] for r in results) / makespan,
+                       "walk_steps_per_s": st["walk_steps"] / makespan, "makespan_s": makespan},
+        "accuracy": {"median_mse_over_target2": float(np.median(mse_ratio)),
+                     "p99_mse_over_target2": float(np.percentile(mse_ratio, 99)),
+                     "done": int(sum(r["state"] == 2 for r in results)),
+                     "capped": int(sum(r["state"] == 3 for r in results))},
+        "server": st, "clocks": clocks.summary(),
+        "gpu_launches": int(st["ticks"]) * 2,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,13 +574,27 @@ def main():
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N slice points (smaller workload for profiler captures; "
                          "the default 0 runs the full slice)")
-    ap.add_argument("--workload", default="slice", choices=["slice", "batch"],
-                    help="slice: the headline Poisson slice (default); batch: 64 batched Laplace instances")
+    ap.add_argument("--workload", default="slice", choices=["slice", "batch", "serve"],
+                    help="slice: the headline Poisson slice (default); batch: 64 batched Laplace instances; "
+                         "serve: the serving loop under Poisson arrivals")
+    ap.add_argument("--serve-requests", type=int, default=600)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
+    ap.add_argument("--serve-large-fraction", type=float, default=0.05)
+    ap.add_argument("--serve-large-max", type=int, default=16384)
+    ap.add_argument("--serve-poisson-fraction", type=float, default=0.25)
+    ap.add_argument("--serve-max-walks", type=int, default=1 << 16)
+    ap.add_argument("--serve-time-limit", type=float, default=150.0)
+    ap.add_argument("--serve-source-samples", type=int, default=16,
+                    help="Green's-function source samples per ball of the Poisson problem")
+    ap.add_argument("--serve-tick-walks", type=int, default=1 << 21)
+    ap.add_argument("--serve-seed", type=int, default=4242)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

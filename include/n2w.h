@@ -589,14 +589,19 @@ typedef struct n2w_server_options {
   int32_t regen_threshold; /* default 8 */
 } n2w_server_options;
 
+#define N2W_STDERR_MAX 0 /* every point's standard error <= target */
+#define N2W_STDERR_RMS 1 /* root mean square over points of the standard errors <= target */
+
 typedef struct n2w_request {
   int32_t mesh;                /* index into the server's meshes */
   int32_t problem;             /* index into the server's problems */
   int64_t point_count;
-  float target_stderr;         /* stop when max over points of the standard error <= this */
+  float target_stderr;         /* stop when the standard error (see stderr_norm) <= this */
   int32_t min_walks_per_point; /* first sweep size floor (>= 32 walks are used) */
   int32_t max_walks_per_point; /* walk cap per point */
   uint64_t seed;
+  int32_t stderr_norm;         /* N2W_STDERR_MAX (default) or N2W_STDERR_RMS */
+  int32_t reserved;
 } n2w_request;
 
 typedef struct n2w_request_info {
@@ -605,6 +610,7 @@ typedef struct n2w_request_info {
   int64_t walks_per_point;  /* walks each point received */
   int64_t ticks;            /* launches the request took part in */
   float max_stderr;         /* max per-point standard error at the end */
+  float rms_stderr;         /* root mean square of the per-point standard errors at the end */
   double queue_seconds;     /* submission -> admission */
   double latency_seconds;   /* submission -> result ready */
 } n2w_request_info;

@@ -10,14 +10,16 @@
 //    request path never calls cudaMalloc.  Requests larger than the whole
 //    pool are refused at submission.
 //  * Ticks.  Each tick is ONE persistent walker launch over every in-flight
-//    request (the batched walker of batch.cu): a walk budget is shared out by
-//    water-filling, each request contributes its next range of points with
+//    request (the batched walker of batch.cu): a walk budget is handed out
+//    shortest-remaining-work first (every request still advances by at least
+//    one point per tick), each request contributes its next range of points with
 //    its current sweep's walks per point, and requests admitted during a tick
 //    join the next one.  Small requests therefore overlap with large ones
 //    instead of queueing behind them.
 //  * Adaptive sweeps.  A sweep gives every point of a request the same number
-//    of walks; after each sweep the maximum per-point standard error is
-//    reduced on the device and the next sweep is sized from it
+//    of walks; after each sweep the maximum (or root mean square, per request)
+//    of the per-point standard errors is reduced on the device and the next
+//    sweep is sized from it
 //    (N_needed = N_done * (stderr / target)^2, plus 10 %), until the target or
 //    the walk cap is met.
 //  * Determinism.  Walk w of point p in sweep s of a request is keyed by
@@ -58,24 +60,35 @@ int64_t now_ns() {
 }
 
 // Max over points of the standard error sqrt(var / n) (float bits; values >= 0
-// order like their bit patterns), written with one atomic per warp.
-__global__ void max_stderr_kernel(const double* __restrict__ sum, const double* __restrict__ sum_sq,
-                                  const uint32_t* __restrict__ count, int64_t n, unsigned* __restrict__ out) {
+// order like their bit patterns) and the sum of var / n, one atomic each per warp.
+__global__ void stderr_kernel(const double* __restrict__ sum, const double* __restrict__ sum_sq,
+                              const uint32_t* __restrict__ count, int64_t n, unsigned* __restrict__ max_out,
+                              double* __restrict__ sum_out) {
   float m = 0.0f;
+  double v2 = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double c = count[i];
     float se = INFINITY;
+    double ev = INFINITY;
     if (c >= 2.0) {
       const double mean = sum[i] / c;
       const double var = fmax(0.0, (sum_sq[i] - c * mean * mean) / (c - 1.0));
-      se = static_cast<float>(sqrt(var / c));
+      ev = var / c;
+      se = static_cast<float>(sqrt(ev));
     }
     m = fmaxf(m, se);
+    v2 += ev;
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(max_out, __float_as_uint(m));
+    atomicAdd(sum_out, v2);
+  }
 }
 
 // First-fit allocator over offsets of one device pool (256-byte granules).
@@ -150,6 +163,7 @@ struct n2w_server {
     int sweep_walks = 0;        // walks per point of the current sweep
     int64_t walks_done = 0;     // walks per point completed
     float max_stderr = INFINITY;
+    float rms_stderr = INFINITY;
     int ticks = 0;
     // results
     std::vector<double> mean, stderr_;
@@ -172,6 +186,8 @@ struct n2w_server {
   char* d_hdr = nullptr;         // queue counter + run counters of a tick
   unsigned* d_conv = nullptr;    // per-slot max stderr (float bits)
   unsigned* h_conv = nullptr;    // pinned
+  double* d_conv_sum = nullptr;  // per-slot sum over points of var / n
+  double* h_conv_sum = nullptr;  // pinned
   n2w_walk_counters* h_counters = nullptr;  // pinned
 
   std::mutex mu;
@@ -263,28 +279,21 @@ void tick(n2w_server& s) {
     for (int64_t id : s.active) act.push_back(s.requests.at(id).get());
   }
   if (act.empty()) return;
-  // Water-filling of the tick's walk budget over the requests' remaining sweep work.
+  // The tick's walk budget goes to the requests with the least remaining
+  // sweep work first (shortest remaining work first keeps small requests
+  // fast); below, every request still advances by at least one point per tick.
   const int64_t budget = s.opt.tick_walks;
   std::vector<int64_t> want(act.size()), give(act.size(), 0);
+  std::vector<size_t> order(act.size());
   for (size_t k = 0; k < act.size(); ++k) {
     want[k] = (act[k]->req.point_count - act[k]->cursor) * static_cast<int64_t>(act[k]->sweep_walks);
+    order[k] = k;
   }
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return want[a] < want[b]; });
   int64_t left = budget;
-  std::vector<size_t> open;
-  for (size_t k = 0; k < act.size(); ++k) open.push_back(k);
-  while (!open.empty() && left > 0) {
-    const int64_t share = std::max<int64_t>(1, left / static_cast<int64_t>(open.size()));
-    std::vector<size_t> still;
-    int64_t used = 0;
-    for (size_t k : open) {
-      const int64_t g = std::min(want[k] - give[k], share);
-      give[k] += g;
-      used += g;
-      if (give[k] < want[k]) still.push_back(k);
-    }
-    left -= used;
-    if (still.size() == open.size() && used == 0) break;
-    open.swap(still);
+  for (size_t k : order) {
+    give[k] = std::min(want[k], left);
+    left -= give[k];
   }
   std::vector<Slice> slices;
   int64_t tick_points = 0;
@@ -353,13 +362,17 @@ void tick(n2w_server& s) {
   }
   if (!swept.empty()) {
     N2W_CUDA(cudaMemsetAsync(s.d_conv, 0, sizeof(unsigned) * swept.size(), st));
+    N2W_CUDA(cudaMemsetAsync(s.d_conv_sum, 0, sizeof(double) * swept.size(), st));
     for (size_t i = 0; i < swept.size(); ++i) {
       const int64_t n = swept[i]->req.point_count;
       const int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 1024));
-      max_stderr_kernel<<<grid, 256, 0, st>>>(swept[i]->sum, swept[i]->sum_sq, swept[i]->count, n, s.d_conv + i);
+      stderr_kernel<<<grid, 256, 0, st>>>(swept[i]->sum, swept[i]->sum_sq, swept[i]->count, n, s.d_conv + i,
+                                          s.d_conv_sum + i);
       N2W_CUDA(cudaGetLastError());
     }
     N2W_CUDA(cudaMemcpyAsync(s.h_conv, s.d_conv, sizeof(unsigned) * swept.size(), cudaMemcpyDeviceToHost, st));
+    N2W_CUDA(cudaMemcpyAsync(s.h_conv_sum, s.d_conv_sum, sizeof(double) * swept.size(), cudaMemcpyDeviceToHost,
+                             st));
   }
   N2W_CUDA(cudaStreamSynchronize(st));
   {
@@ -376,9 +389,12 @@ void tick(n2w_server& s) {
   // Sweep bookkeeping and completion.
   for (size_t i = 0; i < swept.size(); ++i) {
     auto* r = swept[i];
-    float se;
-    std::memcpy(&se, &s.h_conv[i], sizeof(float));
-    r->max_stderr = se;
+    float mx;
+    std::memcpy(&mx, &s.h_conv[i], sizeof(float));
+    r->max_stderr = mx;
+    r->rms_stderr = static_cast<float>(std::sqrt(s.h_conv_sum[i] / static_cast<double>(r->req.point_count)));
+    // the norm the request asked for drives both stopping and the next sweep's size
+    const float se = r->req.stderr_norm == N2W_STDERR_RMS ? r->rms_stderr : r->max_stderr;
     r->walks_done += r->sweep_walks;
     r->cursor = 0;
     r->sweep += 1;
@@ -470,6 +486,8 @@ void destroy_server(n2w_server* s) {
   cudaFree(s->d_problems);
   cudaFreeHost(s->h_insts);
   cudaFreeHost(s->h_conv);
+  cudaFree(s->d_conv_sum);
+  cudaFreeHost(s->h_conv_sum);
   cudaFreeHost(s->h_counters);
   if (s->stream) cudaStreamDestroy(s->stream);
   if (s->scene) {
@@ -545,6 +563,8 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     N2W_CUDA(cudaMalloc(&s->d_hdr, 512));
     N2W_CUDA(cudaMalloc(&s->d_conv, sizeof(unsigned) * o.max_inflight));
     N2W_CUDA(cudaMallocHost(&s->h_conv, sizeof(unsigned) * o.max_inflight));
+    N2W_CUDA(cudaMalloc(&s->d_conv_sum, sizeof(double) * o.max_inflight));
+    N2W_CUDA(cudaMallocHost(&s->h_conv_sum, sizeof(double) * o.max_inflight));
     N2W_CUDA(cudaMallocHost(&s->h_counters, sizeof(n2w_walk_counters)));
     N2W_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->worker = std::thread(worker_loop, s);
@@ -562,6 +582,7 @@ int n2w_server_submit(n2w_server* s, const n2w_request* req, const float* h_poin
                 "problem index out of range");
     N2W_REQUIRE(req->point_count > 0 && h_points, "a request needs at least one point");
     N2W_REQUIRE(req->target_stderr > 0.0f, "target_stderr must be positive");
+    N2W_REQUIRE(req->stderr_norm == N2W_STDERR_MAX || req->stderr_norm == N2W_STDERR_RMS, "bad stderr_norm");
     N2W_REQUIRE(req->max_walks_per_point >= 1 && req->min_walks_per_point >= 0 &&
                     req->min_walks_per_point <= req->max_walks_per_point,
                 "need 0 <= min_walks_per_point <= max_walks_per_point, max >= 1");
@@ -618,6 +639,7 @@ int n2w_server_wait(n2w_server* s, int64_t id, double timeout_seconds, double* h
       info->sweeps = r->sweep;
       info->ticks = r->ticks;
       info->max_stderr = r->max_stderr;
+      info->rms_stderr = r->rms_stderr;
       info->queue_seconds = (r->t_admit ? r->t_admit - r->t_submit : 0) * 1e-9;
       info->latency_seconds = (r->t_finish - r->t_submit) * 1e-9;
     }

@@ -592,11 +592,13 @@ class Server:
         self._sizes = {}
 
     def submit(self, mesh: int, problem: int, points: np.ndarray, target_stderr: float, seed: int = 1,
-               min_walks: int = 32, max_walks: int = 1 << 16) -> int:
+               min_walks: int = 32, max_walks: int = 1 << 16, rms: bool = False) -> int:
+        """rms=False: every point meets the target; rms=True: the root mean
+        square of the per-point standard errors does."""
         from ._lib import Request
 
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
-        r = Request(mesh, problem, len(pts), target_stderr, min_walks, max_walks, seed)
+        r = Request(mesh, problem, len(pts), target_stderr, min_walks, max_walks, seed, 1 if rms else 0, 0)
         rid = C.c_int64()
         call("n2w_server_submit", self._h, C.byref(r), _ptr(pts), C.byref(rid))
         self._sizes[rid.value] = len(pts)
@@ -610,11 +612,12 @@ class Server:
     def wait(self, rid: int, timeout: float = -1.0):
         from ._lib import RequestInfo
 
-        n = self._sizes.pop(rid)
+        n = self._sizes[rid]
         mean = np.empty(n, np.float64)
         se = np.empty(n, np.float64)
         info = RequestInfo()
         call("n2w_server_wait", self._h, rid, C.c_double(timeout), _ptr(mean), _ptr(se), C.byref(info))
+        del self._sizes[rid]  # collected (a timeout leaves the request pending)
         return mean, se, {f: getattr(info, f) for f, _ in RequestInfo._fields_}
 
     def stats(self) -> dict:

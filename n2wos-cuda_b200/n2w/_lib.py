@@ -129,12 +129,14 @@ class ServerOptions(C.Structure):
 class Request(C.Structure):
     _fields_ = [("mesh", C.c_int32), ("problem", C.c_int32), ("point_count", C.c_int64),
                 ("target_stderr", C.c_float), ("min_walks_per_point", C.c_int32),
-                ("max_walks_per_point", C.c_int32), ("seed", C.c_uint64)]
+                ("max_walks_per_point", C.c_int32), ("seed", C.c_uint64), ("stderr_norm", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class RequestInfo(C.Structure):
     _fields_ = [("state", C.c_int32), ("sweeps", C.c_int32), ("walks_per_point", C.c_int64), ("ticks", C.c_int64),
-                ("max_stderr", C.c_float), ("queue_seconds", C.c_double), ("latency_seconds", C.c_double)]
+                ("max_stderr", C.c_float), ("rms_stderr", C.c_float), ("queue_seconds", C.c_double),
+                ("latency_seconds", C.c_double)]
 
 
 class ServerStats(C.Structure):
