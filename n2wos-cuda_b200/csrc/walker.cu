@@ -143,90 +143,6 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   return v;
 }
 
-// Per-lane state of one closest-point query in flight (stack in local memory).
-struct TravState {
-  int sp;
-  int ref;       // inner node to expand next, or kEmptyChild
-  int leaf_cur;  // next triangle slot of the leaf being tested
-  int leaf_end;
-};
-
-// One unit of traversal work for one lane: test ONE triangle of the current
-// leaf, or expand ONE 4-wide node (same ordering and pruning as
-// dev::traverse: children sorted by box distance, nearest entered, others
-// pushed far-to-near, popped entries re-checked).  Returns false once the
-// query is complete.  Splitting the traversal into equal-sized steps is what
-// lets lanes with short queries move on while others are still searching.
-__device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                                          dev::V3 p, dev::ClosestHit& hit, TravState& t, int2* stack,
-                                          uint32_t& c_nodes, uint32_t& c_tris, bool& overflow) {
-  if (t.leaf_cur >= t.leaf_end && t.ref == kEmptyChild) {
-    bool found = false;
-    while (t.sp > 0) {
-      const int2 e = stack[--t.sp];
-      if (__int_as_float(e.y) <= hit.d2) {
-        if (e.x >= 0) {
-          t.ref = e.x;
-        } else {
-          t.leaf_cur = leaf_first(e.x);
-          t.leaf_end = t.leaf_cur + leaf_count(e.x);
-        }
-        found = true;
-        break;
-      }
-    }
-    if (!found) return false;
-  }
-  if (t.leaf_cur < t.leaf_end) {
-    dev::test_slot(tris, t.leaf_cur, p, hit);
-    ++t.leaf_cur;
-    ++c_tris;
-    return true;
-  }
-  const float4* n = nodes + static_cast<size_t>(t.ref) * 8;
-  const float4 lox = __ldg(n + 0);
-  const float4 hix = __ldg(n + 1);
-  const float4 loy = __ldg(n + 2);
-  const float4 hiy = __ldg(n + 3);
-  const float4 loz = __ldg(n + 4);
-  const float4 hiz = __ldg(n + 5);
-  const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
-  ++c_nodes;
-  float d0 = dev::box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
-  float d1 = dev::box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
-  float d2 = dev::box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
-  float d3 = dev::box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
-  int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
-  dev::cswap(d0, r0, d1, r1);
-  dev::cswap(d2, r2, d3, r3);
-  dev::cswap(d0, r0, d2, r2);
-  dev::cswap(d1, r1, d3, r3);
-  dev::cswap(d1, r1, d2, r2);
-  const float best = hit.d2;
-  if (d3 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r3, __float_as_int(d3));
-    else overflow = true;
-  }
-  if (d2 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r2, __float_as_int(d2));
-    else overflow = true;
-  }
-  if (d1 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r1, __float_as_int(d1));
-    else overflow = true;
-  }
-  t.ref = kEmptyChild;
-  if (d0 <= best) {
-    if (r0 >= 0) {
-      t.ref = r0;
-    } else {
-      t.leaf_cur = leaf_first(r0);
-      t.leaf_end = t.leaf_cur + leaf_count(r0);
-    }
-  }
-  return true;
-}
-
 // Persistent walker: a two-phase loop per warp.
 //  Phase A (warp-uniform): finished queries are consumed — the walk stops and
 //    is scored, or moves to its next ball and seeds its next query; finished
@@ -260,7 +176,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
   hit.id = INT32_MAX;
   hit.slot = 0;
   hit.cp = x;
-  TravState tv{0, kEmptyChild, 0, 0};
+  dev::TravState tv{0, kEmptyChild, 0, 0};
   int2 stack[kTraversalStack];
 
   double acc_s = 0.0, acc_s2 = 0.0;
@@ -501,7 +417,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
       if (busy == 0 || __popc(waiting) >= a.regen) break;
       if (querying) {
         bool ov = false;
-        if (!trav_step(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
+        if (!dev::trav_step(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
         if (ov) {
           w_overflow = true;
           ++c_overflow;
