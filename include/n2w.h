@@ -189,8 +189,13 @@ int n2w_bvh_copy_layout(const n2w_bvh* bvh, void* nodes_out, void* tris_out);
 #define N2W_BC_TEXTURE_CHECKER_K8 10
 #define N2W_BC_TEXTURE_CHECKER_K16 11
 #define N2W_BC_CONSTANT_ONE 12
+#define N2W_BC_HARMONIC_MIXTURE_SMOOTH 13     /* reference include/n2wos/nc_harmonic_mixture.hpp */
+#define N2W_BC_HARMONIC_MIXTURE_FIGLIKE 14
+#define N2W_BC_HARMONIC_MIXTURE_MULTISCALE 15
+#define N2W_BC_HARMONIC_MIXTURE_FIGLIKE_HF 16
 #define N2W_BC_POISSON_MULTISCALE 30
 #define N2W_BC_POISSON_FIGLIKE_HF 31
+#define N2W_BC_POISSON_FIGLIKE_HF_X5 32
 #define N2W_BC_CHARGES_SEEDED 100   /* sum_k a_k / |x - c_k| with a seeded charge set */
 #define N2W_BC_POISSON_SINPROD 101  /* u = sin(w x) sin(w y) sin(w z), f = 3 w^2 u */
 

@@ -38,8 +38,17 @@ const ModeName kModes[] = {
     {N2W_BC_TEXTURE_CHECKER_K8, "boundary_texture_checker_k8", {"texture_checker_k8", "checker8", "checker_k8", nullptr}},
     {N2W_BC_TEXTURE_CHECKER_K16, "boundary_texture_checker_k16", {"texture_checker_k16", "checker16", "checker_k16", nullptr}},
     {N2W_BC_CONSTANT_ONE, "constant_one", {"constant", "one", "const1", nullptr}},
-    {N2W_BC_POISSON_MULTISCALE, "poisson_multiscale", {"manufactured_poisson_multiscale", "poisson_mscale", nullptr}},
+    {N2W_BC_HARMONIC_MIXTURE_SMOOTH, "harmonic_mixture_smooth", {"mixture_smooth", "hm_smooth", "fig_smooth", nullptr}},
+    {N2W_BC_HARMONIC_MIXTURE_FIGLIKE, "harmonic_mixture_figlike",
+     {"mixture_figlike", "hm_figlike", "figlike", "fig1", "fig4", nullptr}},
+    {N2W_BC_HARMONIC_MIXTURE_MULTISCALE, "harmonic_mixture_multiscale",
+     {"mixture_multiscale", "hmix_multiscale", "multiscale", nullptr}},
+    {N2W_BC_HARMONIC_MIXTURE_FIGLIKE_HF, "harmonic_mixture_figlike_hf",
+     {"mixture_figlike_hf", "hmix_figlike_hf", "figlike_hf", "fig_hf", nullptr}},
+    {N2W_BC_POISSON_MULTISCALE, "poisson_multiscale",
+     {"manufactured_poisson_multiscale", "poisson_mscale", "poisson", nullptr}},
     {N2W_BC_POISSON_FIGLIKE_HF, "poisson_figlike_hf", {"manufactured_poisson_figlike_hf", "poisson_hf", nullptr}},
+    {N2W_BC_POISSON_FIGLIKE_HF_X5, "poisson_figlike_hf_x5", {"poisson_hf_x5", "poisson_figlike_x5", nullptr}},
     {N2W_BC_CHARGES_SEEDED, "charges_seeded", {"charges8_seeded", "seeded_charges", nullptr}},
     {N2W_BC_POISSON_SINPROD, "poisson_sinprod", {"sinprod", "manufactured_poisson_sinprod", nullptr}},
 };
@@ -127,7 +136,8 @@ int n2w_problem_sinprod(float omega, int source_sampling, n2w_problem* out) {
 int n2w_problem_reference_mode(int mode, int source_sampling, n2w_problem* out) {
   return guarded([&] {
     N2W_REQUIRE(out, "null output");
-    const bool ok = (mode >= 0 && mode <= 12) || mode == N2W_BC_POISSON_MULTISCALE || mode == N2W_BC_POISSON_FIGLIKE_HF;
+    const bool ok = (mode >= 0 && mode <= 16) || mode == N2W_BC_POISSON_MULTISCALE || mode == N2W_BC_POISSON_FIGLIKE_HF ||
+                    mode == N2W_BC_POISSON_FIGLIKE_HF_X5;
     N2W_REQUIRE(ok, "mode " + std::to_string(mode) + " is not a supported reference mode");
     N2W_REQUIRE(source_sampling == N2W_SOURCE_BALL || source_sampling == N2W_SOURCE_CENTER, "bad source_sampling");
     std::memset(out, 0, sizeof(*out));

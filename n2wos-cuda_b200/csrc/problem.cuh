@@ -116,6 +116,92 @@ N2W_PHD void poisson_figlike_hf(T x, T y, T z, T& u, T& f) {
   u += T(0.08) * x + T(0.05) * y - T(0.03) * z;
 }
 
+// One harmonic term A exp(k a.x) {cos|sin}(k b.x + phi) with a, b orthonormal:
+// the exponential's second derivative along a cancels the oscillation's along
+// b.  The reference's analytic mixtures (include/n2wos/nc_harmonic_mixture.hpp)
+// are scaled sums of such terms plus a linear part; their coefficient tables
+// are kept as given there so the boundary data are the same functions.
+template <typename T>
+N2W_PHD T harmonic_term(T x, T y, T z, T amp, T k, T ax, T ay, T az, T bx, T by, T bz, T phi, bool use_sin) {
+  const T adot = ax * x + ay * y + az * z;
+  const T arg = k * (bx * x + by * y + bz * z) + phi;
+  return amp * Math<T>::e(k * adot) * (use_sin ? Math<T>::s(arg) : Math<T>::c(arg));
+}
+
+template <typename T>
+N2W_PHD T harmonic_mixture(T x, T y, T z, int mode) {
+  const T r = T(0.70710678118), s3 = T(0.57735026919);
+  T t = T(0), lin = T(0), scale = T(1);
+  switch (mode) {
+    case N2W_BC_HARMONIC_MIXTURE_SMOOTH:
+      t += harmonic_term<T>(x, y, z, T(0.42), T(1.15), T(1), T(0), T(0), T(0), T(1), T(0), T(0.15), false);
+      t += harmonic_term<T>(x, y, z, T(-0.30), T(1.05), T(0), T(-1), T(0), T(0), T(0), T(1), T(-0.25), true);
+      t += harmonic_term<T>(x, y, z, T(0.24), T(1.25), T(0.6), T(0), T(0.8), T(-0.8), T(0), T(0.6), T(0.70), false);
+      t += harmonic_term<T>(x, y, z, T(0.18), T(1.10), -s3, -s3, -s3, r, -r, T(0), T(1.10), true);
+      lin = T(0.12) * x - T(0.08) * y + T(0.06) * z;
+      scale = T(0.72);
+      break;
+    case N2W_BC_HARMONIC_MIXTURE_FIGLIKE:
+      t += harmonic_term<T>(x, y, z, T(0.36), T(1.65), T(1), T(0), T(0), T(0), T(1), T(0), T(0.35), false);
+      t += harmonic_term<T>(x, y, z, T(-0.30), T(1.45), T(0), T(-1), T(0), T(0), T(0), T(1), T(-0.20), false);
+      t += harmonic_term<T>(x, y, z, T(0.27), T(1.85), r, T(0), r, -r, T(0), r, T(0.55), true);
+      t += harmonic_term<T>(x, y, z, T(0.18), T(1.30), T(0), T(-0.8), T(-0.6), T(0), T(-0.6), T(0.8), T(-0.90),
+                            false);
+      lin = T(0.10) * x + T(0.14) * y - T(0.05) * z;
+      scale = T(0.58);
+      break;
+    case N2W_BC_HARMONIC_MIXTURE_MULTISCALE:
+      t += harmonic_term<T>(x, y, z, T(0.20), T(1.35), T(1), T(0), T(0), T(0), T(1), T(0), T(0.20), false);
+      t += harmonic_term<T>(x, y, z, T(-0.17), T(1.55), T(0), T(-1), T(0), T(0), T(0), T(1), T(-0.45), true);
+      t += harmonic_term<T>(x, y, z, T(0.15), T(1.70), T(0), T(0), T(1), T(1), T(0), T(0), T(0.80), false);
+      t += harmonic_term<T>(x, y, z, T(0.095), T(2.55), r, r, T(0), -r, r, T(0), T(0.15), false);
+      t += harmonic_term<T>(x, y, z, T(-0.080), T(2.85), T(0), -r, -r, T(0), -r, r, T(-0.65), true);
+      t += harmonic_term<T>(x, y, z, T(0.070), T(3.15), r, T(0), r, -r, T(0), r, T(1.10), false);
+      t += harmonic_term<T>(x, y, z, T(0.060), T(3.35), -s3, -s3, -s3, r, -r, T(0), T(0.40), true);
+      t += harmonic_term<T>(x, y, z, T(0.035), T(4.00), T(0.81649658093), T(-0.40824829046), T(-0.40824829046),
+                            T(0), r, -r, T(-0.35), false);
+      lin = T(0.035) * x - T(0.025) * y + T(0.020) * z;
+      scale = T(0.62);
+      break;
+    default:  // N2W_BC_HARMONIC_MIXTURE_FIGLIKE_HF
+      t += harmonic_term<T>(x, y, z, T(0.18), T(1.65), T(1), T(0), T(0), T(0), T(1), T(0), T(0.35), false);
+      t += harmonic_term<T>(x, y, z, T(-0.15), T(1.75), T(0), T(-1), T(0), T(0), T(0), T(1), T(-0.20), false);
+      t += harmonic_term<T>(x, y, z, T(0.13), T(1.85), T(0), T(0), T(1), T(1), T(0), T(0), T(0.70), true);
+      t += harmonic_term<T>(x, y, z, T(0.095), T(2.90), r, T(0), r, -r, T(0), r, T(0.55), true);
+      t += harmonic_term<T>(x, y, z, T(-0.085), T(3.25), -r, -r, T(0), -r, r, T(0), T(-0.75), false);
+      t += harmonic_term<T>(x, y, z, T(0.070), T(3.55), T(0), r, r, T(0), -r, r, T(1.20), true);
+      t += harmonic_term<T>(x, y, z, T(0.040), T(4.20), T(0.86602540378), T(0), T(0.5), T(-0.5), T(0),
+                            T(0.86602540378), T(0.25), false);
+      t += harmonic_term<T>(x, y, z, T(-0.032), T(4.50), T(0), T(-0.8), T(-0.6), T(0), T(-0.6), T(0.8), T(-0.30), true);
+      lin = T(0.025) * x + T(0.020) * y - T(0.015) * z;
+      scale = T(0.55);
+      break;
+  }
+  return scale * (t + lin);
+}
+
+// Higher-frequency manufactured Poisson field of the reference
+// (include/n2wos/nc_poisson_manufactured.hpp:160-209): a Fourier mixture
+// u = sum A trig(k.x + phi) + a weak linear part, f = -Lap u = sum A |k|^2 trig(...).
+template <typename T>
+N2W_PHD void fourier_term(T x, T y, T z, T amp, T kx, T ky, T kz, T phi, bool use_sin, T& u, T& f) {
+  const T arg = kx * x + ky * y + kz * z + phi;
+  const T v = amp * (use_sin ? Math<T>::s(arg) : Math<T>::c(arg));
+  u += v;
+  f += (kx * kx + ky * ky + kz * kz) * v;
+}
+
+template <typename T>
+N2W_PHD void poisson_figlike_hf_x5(T x, T y, T z, T& u, T& f) {
+  fourier_term<T>(x, y, z, T(0.090), T(12.0), T(4.0), T(1.5), T(0.30), true, u, f);
+  fourier_term<T>(x, y, z, T(0.075), T(-5.0), T(13.5), T(2.0), T(-0.70), false, u, f);
+  fourier_term<T>(x, y, z, T(0.060), T(7.5), T(-3.5), T(15.0), T(1.10), true, u, f);
+  fourier_term<T>(x, y, z, T(0.050), T(14.0), T(-10.0), T(4.0), T(2.20), false, u, f);
+  fourier_term<T>(x, y, z, T(0.045), T(-9.0), T(6.5), T(12.0), T(-1.30), true, u, f);
+  fourier_term<T>(x, y, z, T(0.035), T(18.0), T(2.5), T(-7.0), T(0.80), false, u, f);
+  u += T(0.030) * (T(0.60) * x - T(0.35) * y + T(0.20) * z);
+}
+
 // Fixed charge sets of the reference (cubql_bvh.cu:1266-1296).
 template <typename T>
 N2W_PHD T fixed_charges(T x, T y, T z, int mode) {
@@ -163,6 +249,15 @@ N2W_PHD T problem_u(const n2w_problem& pb, T x, T y, T z) {
     case N2W_BC_TEXTURE_CHECKER_K8: return texture_checker<T>(x, y, z, 8);
     case N2W_BC_TEXTURE_CHECKER_K16: return texture_checker<T>(x, y, z, 16);
     case N2W_BC_CONSTANT_ONE: return T(1);
+    case N2W_BC_HARMONIC_MIXTURE_SMOOTH:
+    case N2W_BC_HARMONIC_MIXTURE_FIGLIKE:
+    case N2W_BC_HARMONIC_MIXTURE_MULTISCALE:
+    case N2W_BC_HARMONIC_MIXTURE_FIGLIKE_HF: return harmonic_mixture<T>(x, y, z, pb.mode);
+    case N2W_BC_POISSON_FIGLIKE_HF_X5: {
+      T u = T(0), f = T(0);
+      poisson_figlike_hf_x5<T>(x, y, z, u, f);
+      return u;
+    }
     case N2W_BC_POISSON_MULTISCALE: {
       T u = T(0), f = T(0);
       poisson_multiscale<T>(x, y, z, u, f);
@@ -207,13 +302,18 @@ N2W_PHD T problem_f(const n2w_problem& pb, T x, T y, T z) {
       const T w = T(pb.omega);
       return T(3) * w * w * Math<T>::s(w * x) * Math<T>::s(w * y) * Math<T>::s(w * z);
     }
+    case N2W_BC_POISSON_FIGLIKE_HF_X5: {
+      T u = T(0), f = T(0);
+      poisson_figlike_hf_x5<T>(x, y, z, u, f);
+      return f;
+    }
     default: return T(0);
   }
 }
 
 N2W_PHD bool problem_has_source(const n2w_problem& pb) {
   return pb.mode == N2W_BC_POISSON_MULTISCALE || pb.mode == N2W_BC_POISSON_FIGLIKE_HF ||
-         pb.mode == N2W_BC_POISSON_SINPROD;
+         pb.mode == N2W_BC_POISSON_FIGLIKE_HF_X5 || pb.mode == N2W_BC_POISSON_SINPROD;
 }
 
 // Whether u is a known solution in the interior (false for the texture modes,

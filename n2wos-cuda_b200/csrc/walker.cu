@@ -637,8 +637,8 @@ void validate_walk_options(const n2w_walk_options& o) {
 
 void validate_problem(const n2w_problem& p) {
   const int m = p.mode;
-  const bool ok = (m >= 0 && m <= 12) || m == N2W_BC_POISSON_MULTISCALE || m == N2W_BC_POISSON_FIGLIKE_HF ||
-                  m == N2W_BC_CHARGES_SEEDED || m == N2W_BC_POISSON_SINPROD;
+  const bool ok = (m >= 0 && m <= 16) || m == N2W_BC_POISSON_MULTISCALE || m == N2W_BC_POISSON_FIGLIKE_HF ||
+                  m == N2W_BC_POISSON_FIGLIKE_HF_X5 || m == N2W_BC_CHARGES_SEEDED || m == N2W_BC_POISSON_SINPROD;
   N2W_REQUIRE(ok, "unsupported boundary mode " + std::to_string(m));
   N2W_REQUIRE(p.source_sampling == N2W_SOURCE_BALL || p.source_sampling == N2W_SOURCE_CENTER,
               "source_sampling must be N2W_SOURCE_BALL or N2W_SOURCE_CENTER");

@@ -27,7 +27,9 @@ N2W_BC = {
     "external_charges_shell_k8": 6, "external_charges_shell_k16": 7,
     "boundary_texture_stripes_k8": 8, "boundary_texture_stripes_k16": 9,
     "boundary_texture_checker_k8": 10, "boundary_texture_checker_k16": 11,
-    "constant_one": 12, "poisson_multiscale": 30, "poisson_figlike_hf": 31,
+    "constant_one": 12, "harmonic_mixture_smooth": 13, "harmonic_mixture_figlike": 14,
+    "harmonic_mixture_multiscale": 15, "harmonic_mixture_figlike_hf": 16,
+    "poisson_multiscale": 30, "poisson_figlike_hf": 31, "poisson_figlike_hf_x5": 32,
     "charges_seeded": 100, "poisson_sinprod": 101,
 }
 N2W_SOURCE_BALL, N2W_SOURCE_CENTER = 0, 1

@@ -58,7 +58,18 @@ def ref():
         _ref.ref_count_degenerate.argtypes = [C.c_void_p]
         _ref.ref_host_bvh_stats.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         _ref.ref_last_error.restype = C.c_char_p
+        _ref.ref_analytic_mode.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     return _ref
+
+
+def ref_analytic(mode: int, points):
+    """u and f of the reference's header-only analytic modes (13-16, 30-32)."""
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    u = np.empty(len(pts), np.float32)
+    f = np.empty(len(pts), np.float32)
+    if ref().ref_analytic_mode(mode, _p(pts), len(pts), _p(u), _p(f)) != 0:
+        raise ValueError(f"mode {mode} is not an analytic reference mode")
+    return u, f
 
 
 class RefMesh:

@@ -11,6 +11,8 @@
 #include "n2wos/closest_point.hpp"
 #include "n2wos/cuda_bvh.hpp"
 #include "n2wos/mesh.hpp"
+#include "n2wos/nc_harmonic_mixture.hpp"
+#include "n2wos/nc_poisson_manufactured.hpp"
 
 namespace {
 thread_local std::string g_err;
@@ -120,6 +122,38 @@ int ref_host_bvh_stats(void* h, int leaf_size, int64_t* nodes, int32_t* depth) {
     g_err = e.what();
     return 1;
   }
+}
+
+// Boundary data u and source f of the reference's header-only analytic modes
+// (harmonic mixtures 13-16, manufactured Poisson 30, 31, 32), evaluated by the
+// reference's own inline functions.  Returns 0, or -1 for another mode.
+struct RefP {
+  float x, y, z;
+};
+int ref_analytic_mode(int mode, const float* xyz, int64_t n, float* u_out, float* f_out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const RefP p{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    float u = 0.0f, f = 0.0f;
+    switch (mode) {
+      case 13: u = n2wos::nc_harmonic_mixture_smooth_value(p); break;
+      case 14: u = n2wos::nc_harmonic_mixture_figlike_value(p); break;
+      case 15: u = n2wos::nc_harmonic_mixture_multiscale_value(p); break;
+      case 16: u = n2wos::nc_harmonic_mixture_figlike_hf_value(p); break;
+      case 30:
+      case 31:
+        u = n2wos::nc_poisson_manufactured_u(p, mode);
+        f = n2wos::nc_poisson_manufactured_f(p, mode);
+        break;
+      case 32:
+        u = ::nc_poisson_figlike_hf_x5_value(p);  // declared outside namespace n2wos
+        f = ::nc_poisson_figlike_hf_x5_source(p);
+        break;
+      default: return -1;
+    }
+    u_out[i] = u;
+    f_out[i] = f;
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -7,6 +7,8 @@ tests (CPU and GPU) read without the reference.
 Fixtures:
 * bumpy_ref_16x32.npz — the reference generator's bumpy sphere (stacks 16,
   slices 32, amplitude 0.15), raw and normalised, with the normalisation.
+* analytic_modes.npz — u and f of the reference's analytic modes 13-16 and
+  30-32 (its header functions) at 256 seeded points;
 * mesh_hashes.json — SHA-256 of the reference generator's normalised
   128x256 bumpy sphere (vertices float32 bytes, triangles uint32 bytes) and of
   the reference PLY loader's output for the bundled bunny mesh.
@@ -84,6 +86,12 @@ def main() -> None:
     pts = query_points(v.astype(np.float64), t)
     d2, cp, ids = big.bruteforce(pts)
     np.savez_compressed(HERE / "closest_golden.npz", points=pts, distance2=d2, closest=cp, triangle_id=ids)
+    ap = np.random.default_rng(2024).uniform(-1.1, 1.1, (256, 3)).astype(np.float32)
+    modes = {}
+    for mode in (13, 14, 15, 16, 30, 31, 32):
+        u, f = oracle.ref_analytic(mode, ap)
+        modes[f"u_{mode}"], modes[f"f_{mode}"] = u, f
+    np.savez_compressed(HERE / "analytic_modes.npz", points=ap, **modes)
     print("wrote golden fixtures to", HERE)
 
 

@@ -236,3 +236,15 @@ def test_invalid_options(gpu, small_scene):
         run(gpu, bvh, bad, pts)
     r, cnt = run(gpu, bvh, p, pts[:0])
     assert len(r["mean"]) == 0
+
+
+@pytest.mark.parametrize("name", ["harmonic_mixture_figlike", "harmonic_mixture_figlike_hf", "poisson_figlike_hf_x5"])
+def test_reference_analytic_modes_walk_to_exact(gpu, small_scene, name):
+    """The reference's analytic mixtures (13-16) and the x5 Poisson field (32):
+    plain WoS converges to the FP64 solution (centre source rule as the reference)."""
+    m, bvh, nodes, tris, pts = small_scene
+    p = gpu.problem_reference(gpu.N2W_BC[name], gpu.N2W_SOURCE_BALL)
+    r, cnt = run(gpu, bvh, p, pts, walks_per_point=4096, epsilon=1e-4, seed=3)
+    assert cnt["overflow"] == 0
+    exact = gpu.problem_exact(p, pts.astype(np.float64))
+    assert np.all(np.abs(r["mean"] - exact) <= 4 * r["stderr"] + 2e-3), (r["mean"] - exact, r["stderr"])
