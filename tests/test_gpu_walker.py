@@ -241,7 +241,7 @@ def test_invalid_options(gpu, small_scene):
 @pytest.mark.parametrize("name", ["harmonic_mixture_figlike", "harmonic_mixture_figlike_hf", "poisson_figlike_hf_x5"])
 def test_reference_analytic_modes_walk_to_exact(gpu, small_scene, name):
     """The reference's analytic mixtures (13-16) and the x5 Poisson field (32):
-    plain WoS converges to the FP64 solution (centre source rule as the reference)."""
+    plain WoS (in-ball source sampling) converges to the FP64 solution."""
     m, bvh, nodes, tris, pts = small_scene
     p = gpu.problem_reference(gpu.N2W_BC[name], gpu.N2W_SOURCE_BALL)
     r, cnt = run(gpu, bvh, p, pts, walks_per_point=4096, epsilon=1e-4, seed=3)
