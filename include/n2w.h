@@ -606,35 +606,60 @@ typedef struct n2w_request {
   int32_t max_walks_per_point; /* walk cap per point */
   uint64_t seed;
   int32_t stderr_norm;         /* N2W_STDERR_MAX (default) or N2W_STDERR_RMS */
-  int32_t reserved;
+  int32_t mode;                /* N2W_REQUEST_MODE_PLAIN or N2W_REQUEST_MODE_NC2LMC */
 } n2w_request;
+
+#define N2W_REQUEST_MODE_PLAIN 0  /* plain WoS, batched with every plain request of the tick */
+#define N2W_REQUEST_MODE_NC2LMC 1 /* NC+2LMC with the cache registered for (mesh, problem) */
+
+/* A pre-trained cache for NC+2LMC requests on one (mesh, problem) pair.  The
+ * cache must outlive the server.  Each sweep of such a request runs
+ * coarse_walks walks truncated at depth_m and closed by the cache plus
+ * ceil(residual_fraction * coarse_walks) residual walks per point, in chunks
+ * of 4,096 points between the plain ticks (n2w_nc2lmc_estimate_ex; its sample
+ * buffers come from the stream-ordered allocator), so NC walks do not share
+ * the plain requests' launch.  The standard error is sqrt(var_c/N_c + var_r/N_r). */
+typedef struct n2w_server_nc {
+  const n2w_cache* cache;
+  float input_min[3];
+  float input_extent[3];
+  int32_t depth_m;
+  float residual_fraction;
+} n2w_server_nc;
 
 typedef struct n2w_request_info {
   int32_t state;            /* N2W_REQUEST_* */
   int32_t sweeps;
-  int64_t walks_per_point;  /* walks each point received */
-  int64_t ticks;            /* launches the request took part in */
+  int64_t walks_per_point;  /* walks each point received (NC+2LMC: coarse walks) */
+  int64_t ticks;            /* launches the request took part in (NC+2LMC: chunks) */
   float max_stderr;         /* max per-point standard error at the end */
   float rms_stderr;         /* root mean square of the per-point standard errors at the end */
   double queue_seconds;     /* submission -> admission */
   double latency_seconds;   /* submission -> result ready */
+  int64_t residual_walks_per_point; /* NC+2LMC: residual walks each point received */
 } n2w_request_info;
 
 typedef struct n2w_server_stats {
   int64_t submitted, completed, inflight, pending, peak_inflight;
   int64_t ticks, walks, walk_steps, overflow;
   int64_t pool_bytes, pool_used, peak_pool_bytes;
+  int64_t nc_chunks, nc_walks; /* NC+2LMC chunks run and their coarse + residual walks */
 } n2w_server_stats;
 
 typedef struct n2w_server n2w_server;
 int n2w_server_options_default(n2w_server_options* out);
-/* Builds the scene from the BVHs (which may be destroyed afterwards), copies
- * the problems, allocates the pool and starts the worker thread on the
- * current device. */
+/* Builds the scene from the BVHs, copies the problems, allocates the pool and
+ * starts the worker thread on the current device.  The BVHs must outlive the
+ * server (NC+2LMC requests walk them directly). */
 int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_problem* problems, int problem_count,
                       const n2w_server_options* options, n2w_server** out);
+/* Registers (or replaces) the cache used by NC+2LMC requests on (mesh, problem).
+ * nc->cache == NULL selects the analytic cache C(x) = u(x) (a check of the
+ * estimator, as n2w_nc2lmc_estimate_ex).  depth_m >= 0, residual_fraction in (0, 1]. */
+int n2w_server_set_nc(n2w_server* server, int mesh, int problem, const n2w_server_nc* nc);
 /* Thread-safe.  Copies the host points (3 * point_count floats).  Requests
- * larger than the whole pool fail with N2W_ENOMEM. */
+ * larger than the whole pool fail with N2W_ENOMEM; NC+2LMC requests need a
+ * cache registered for their (mesh, problem). */
 int n2w_server_submit(n2w_server* server, const n2w_request* request, const float* h_points, int64_t* id_out);
 int n2w_server_poll(n2w_server* server, int64_t id, int* state_out);
 /* Blocks until the request finishes (timeout_seconds < 0: no limit; on

@@ -27,6 +27,15 @@
 //    and sweep sizes depend only on the request's own statistics, so a
 //    request's estimates are the same alone and in any mix, up to the order of
 //    FP64 additions.
+//  * NC+2LMC requests.  A request in N2W_REQUEST_MODE_NC2LMC uses the cache
+//    registered for its (mesh, problem) with n2w_server_set_nc.  Its sweeps
+//    run between the ticks as fixed chunks of kNcChunk points through
+//    n2w_nc2lmc_estimate_ex on the request's own BVH (coarse walks truncated
+//    at depth m and closed by the cache, plus residual walks), each chunk
+//    keyed by (request seed, sweep, chunk index), so these requests are also
+//    the same alone and in a mix.  The chunk's statistics land in a scratch
+//    area and are added to the request's totals; convergence uses the
+//    estimator's standard error sqrt(var_c / N_c + var_r / N_r).
 //
 // The reference has no serving loop (it evaluates one point set per process);
 // the walk itself is the reference's (src/cuda/cubql_bvh.cu:1323-1357).
@@ -59,25 +68,34 @@ int64_t now_ns() {
       .count();
 }
 
-// Max over points of the standard error sqrt(var / n) (float bits; values >= 0
-// order like their bit patterns) and the sum of var / n, one atomic each per warp.
-__global__ void stderr_kernel(const double* __restrict__ sum, const double* __restrict__ sum_sq,
-                              const uint32_t* __restrict__ count, int64_t n, unsigned* __restrict__ max_out,
+// Variance of the mean of c samples with sum s and sum of squares q (infinite
+// below two samples).
+__host__ __device__ inline double mean_variance(double s, double q, double c) {
+  if (c < 2.0) return INFINITY;
+  const double mean = s / c;
+  return fmax(0.0, (q - c * mean * mean) / (c - 1.0)) / c;
+}
+
+// Per-point sample sums of one estimator level.
+struct LevelSums {
+  double* sum = nullptr;
+  double* sum_sq = nullptr;
+  uint32_t* count = nullptr;
+};
+
+// Max over points of the standard error (float bits; values >= 0 order like
+// their bit patterns) and the sum of the estimator variances, one atomic each
+// per warp.  The variance is var / n of level a, plus that of level b when
+// b.sum is set (NC+2LMC: coarse + residual).
+__global__ void stderr_kernel(LevelSums a, LevelSums b, int64_t n, unsigned* __restrict__ max_out,
                               double* __restrict__ sum_out) {
   float m = 0.0f;
   double v2 = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const double c = count[i];
-    float se = INFINITY;
-    double ev = INFINITY;
-    if (c >= 2.0) {
-      const double mean = sum[i] / c;
-      const double var = fmax(0.0, (sum_sq[i] - c * mean * mean) / (c - 1.0));
-      ev = var / c;
-      se = static_cast<float>(sqrt(ev));
-    }
-    m = fmaxf(m, se);
+    double ev = mean_variance(a.sum[i], a.sum_sq[i], a.count[i]);
+    if (b.sum) ev += mean_variance(b.sum[i], b.sum_sq[i], b.count[i]);
+    m = fmaxf(m, static_cast<float>(sqrt(ev)));
     v2 += ev;
   }
 #pragma unroll
@@ -136,8 +154,45 @@ class PoolAllocator {
 };
 
 // Device bytes a request of n points holds while in flight: points (12 B) and
-// accumulators (sum, sum_sq, steps: 8 B; count, forced: 4 B).
-size_t request_bytes(int64_t n) { return static_cast<size_t>(n) * 44 + 5 * 256; }
+// accumulators (sum, sum_sq, steps: 8 B; count, forced: 4 B); NC+2LMC adds
+// the residual level's sum, sum_sq (8 B) and count (4 B).
+size_t request_bytes(int64_t n, bool nc) {
+  return static_cast<size_t>(n) * (nc ? 64 : 44) + (nc ? 8 : 5) * 256;
+}
+
+// Points per NC+2LMC chunk (the unit of work and of walk keying).
+constexpr int64_t kNcChunk = 4096;
+
+uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Adds one chunk's coarse and residual statistics (scratch, chunk-relative)
+// into a request's totals at point offset `first`.
+struct NcChunkAdd {
+  const double *c_sum, *c_sum_sq, *r_sum, *r_sum_sq;
+  const uint32_t *c_count, *c_forced, *r_count;
+  const uint64_t* c_steps;
+  double *t_c_sum, *t_c_sum_sq, *t_r_sum, *t_r_sum_sq;
+  uint32_t *t_c_count, *t_c_forced, *t_r_count;
+  uint64_t* t_c_steps;
+};
+
+__global__ void add_nc_chunk_kernel(NcChunkAdd a, int64_t n) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a.t_c_sum[i] += a.c_sum[i];
+  a.t_c_sum_sq[i] += a.c_sum_sq[i];
+  a.t_c_count[i] += a.c_count[i];
+  a.t_c_steps[i] += a.c_steps[i];
+  a.t_c_forced[i] += a.c_forced[i];
+  a.t_r_sum[i] += a.r_sum[i];
+  a.t_r_sum_sq[i] += a.r_sum_sq[i];
+  a.t_r_count[i] += a.r_count[i];
+}
 
 }  // namespace
 }  // namespace n2w
@@ -157,6 +212,13 @@ struct n2w_server {
     double *sum = nullptr, *sum_sq = nullptr;
     uint64_t* steps = nullptr;
     uint32_t *count = nullptr, *forced = nullptr;
+    // NC+2LMC: the cache and the residual level (the fields above hold the coarse level)
+    bool nc = false;
+    n2w_server_nc ncfg{};
+    double *r_sum = nullptr, *r_sum_sq = nullptr;
+    uint32_t* r_count = nullptr;
+    int residual_walks = 0;     // residual walks per point of the current sweep
+    int64_t residual_done = 0;  // residual walks per point completed
     // progress
     int64_t cursor = 0;         // next point of the current sweep
     int sweep = 0;              // index of the current sweep
@@ -171,6 +233,8 @@ struct n2w_server {
   };
 
   std::unique_ptr<n2w_scene> scene;
+  std::vector<const n2w_bvh*> bvhs;  // NC+2LMC requests walk the meshes' own BVHs
+  std::map<std::pair<int, int>, n2w_server_nc> nc;  // (mesh, problem) -> cache; guarded by mu
   std::vector<n2w_problem> problems;
   n2w_problem* d_problems = nullptr;
   n2w_server_options opt{};
@@ -189,6 +253,7 @@ struct n2w_server {
   double* d_conv_sum = nullptr;  // per-slot sum over points of var / n
   double* h_conv_sum = nullptr;  // pinned
   n2w_walk_counters* h_counters = nullptr;  // pinned
+  char* d_nc_scratch = nullptr;  // one chunk's coarse + residual statistics
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -203,6 +268,12 @@ struct n2w_server {
 };
 
 namespace {
+
+// Residual walks per point of an NC+2LMC sweep with `coarse` coarse walks (at
+// least two, so that the residual variance is defined after the first sweep).
+int residual_walks_for(const n2w_server_nc& c, int coarse) {
+  return std::max(2, static_cast<int>(std::ceil(static_cast<double>(c.residual_fraction) * coarse)));
+}
 
 void fail_all_locked(n2w_server& s, const std::string& msg) {
   s.fatal = msg;
@@ -229,10 +300,10 @@ void admit(n2w_server& s) {
       auto& r = *s.requests.at(s.pending.front());
       const int64_t n = r.req.point_count;
       size_t off = 0;
-      if (!s.pool->alloc(request_bytes(n), &off)) break;  // head-of-line waits for memory
+      if (!s.pool->alloc(request_bytes(n, r.nc), &off)) break;  // head-of-line waits for memory
       s.pending.pop_front();
       r.pool_off = off;
-      r.pool_len = request_bytes(n);
+      r.pool_len = request_bytes(n, r.nc);
       char* base = s.d_pool + off;
       auto carve = [&](size_t bytes) {
         char* p = base;
@@ -245,9 +316,15 @@ void admit(n2w_server& s) {
       r.count = reinterpret_cast<uint32_t*>(carve(4 * n));
       r.forced = reinterpret_cast<uint32_t*>(carve(4 * n));
       r.d_points = reinterpret_cast<n2w_vec3*>(carve(12 * n));
+      if (r.nc) {
+        r.r_sum = reinterpret_cast<double*>(carve(8 * n));
+        r.r_sum_sq = reinterpret_cast<double*>(carve(8 * n));
+        r.r_count = reinterpret_cast<uint32_t*>(carve(4 * n));
+      }
       r.state = N2W_REQUEST_ACTIVE;
       r.t_admit = now_ns();
       r.sweep_walks = std::min(r.req.max_walks_per_point, std::max(32, r.req.min_walks_per_point));
+      if (r.nc) r.residual_walks = residual_walks_for(r.ncfg, r.sweep_walks);
       s.active.push_back(r.id);
       admitted.push_back(&r);
       s.stats.peak_inflight = std::max<int64_t>(s.stats.peak_inflight, static_cast<int64_t>(s.active.size()));
@@ -261,7 +338,106 @@ void admit(n2w_server& s) {
     N2W_CUDA(cudaMemsetAsync(r->steps, 0, 8 * n, s.stream));
     N2W_CUDA(cudaMemsetAsync(r->count, 0, 4 * n, s.stream));
     N2W_CUDA(cudaMemsetAsync(r->forced, 0, 4 * n, s.stream));
+    if (r->nc) {
+      N2W_CUDA(cudaMemsetAsync(r->r_sum, 0, 8 * n, s.stream));
+      N2W_CUDA(cudaMemsetAsync(r->r_sum_sq, 0, 8 * n, s.stream));
+      N2W_CUDA(cudaMemsetAsync(r->r_count, 0, 4 * n, s.stream));
+    }
     N2W_CUDA(cudaMemcpyAsync(r->d_points, r->h_points.data(), 12 * n, cudaMemcpyHostToDevice, s.stream));
+  }
+}
+
+// Queues the standard-error reduction of every request in `swept` (slot i of
+// d_conv / d_conv_sum) and its copy to the pinned host slots.
+void launch_sweep_stderr(n2w_server& s, const std::vector<n2w_server::Request*>& swept) {
+  const cudaStream_t st = s.stream;
+  N2W_CUDA(cudaMemsetAsync(s.d_conv, 0, sizeof(unsigned) * swept.size(), st));
+  N2W_CUDA(cudaMemsetAsync(s.d_conv_sum, 0, sizeof(double) * swept.size(), st));
+  for (size_t i = 0; i < swept.size(); ++i) {
+    const auto* r = swept[i];
+    const int64_t n = r->req.point_count;
+    const int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 1024));
+    LevelSums a{r->sum, r->sum_sq, r->count}, b{};
+    if (r->nc) b = LevelSums{r->r_sum, r->r_sum_sq, r->r_count};
+    stderr_kernel<<<grid, 256, 0, st>>>(a, b, n, s.d_conv + i, s.d_conv_sum + i);
+    N2W_CUDA(cudaGetLastError());
+  }
+  N2W_CUDA(cudaMemcpyAsync(s.h_conv, s.d_conv, sizeof(unsigned) * swept.size(), cudaMemcpyDeviceToHost, st));
+  N2W_CUDA(cudaMemcpyAsync(s.h_conv_sum, s.d_conv_sum, sizeof(double) * swept.size(), cudaMemcpyDeviceToHost, st));
+}
+
+// Sweep bookkeeping after the stream has synchronised: record the standard
+// errors, then either finish the request (results to the host, pool space
+// released) or size its next sweep.
+void finish_sweeps(n2w_server& s, const std::vector<n2w_server::Request*>& swept) {
+  const cudaStream_t st = s.stream;
+  for (size_t i = 0; i < swept.size(); ++i) {
+    auto* r = swept[i];
+    float mx;
+    std::memcpy(&mx, &s.h_conv[i], sizeof(float));
+    r->max_stderr = mx;
+    r->rms_stderr = static_cast<float>(std::sqrt(s.h_conv_sum[i] / static_cast<double>(r->req.point_count)));
+    // the norm the request asked for drives both stopping and the next sweep's size
+    const float se = r->req.stderr_norm == N2W_STDERR_RMS ? r->rms_stderr : r->max_stderr;
+    r->walks_done += r->sweep_walks;
+    r->residual_done += r->residual_walks;
+    r->cursor = 0;
+    r->sweep += 1;
+    const bool reached = se <= r->req.target_stderr && r->walks_done >= r->req.min_walks_per_point;
+    const bool capped = r->walks_done >= r->req.max_walks_per_point;
+    if (reached || capped) {
+      const int64_t n = r->req.point_count;
+      std::vector<double> sum(n), sum_sq(n), rsum, rsum_sq;
+      std::vector<uint32_t> cnt(n), rcnt;
+      N2W_CUDA(cudaMemcpyAsync(sum.data(), r->sum, 8 * n, cudaMemcpyDeviceToHost, st));
+      N2W_CUDA(cudaMemcpyAsync(sum_sq.data(), r->sum_sq, 8 * n, cudaMemcpyDeviceToHost, st));
+      N2W_CUDA(cudaMemcpyAsync(cnt.data(), r->count, 4 * n, cudaMemcpyDeviceToHost, st));
+      if (r->nc) {
+        rsum.resize(n);
+        rsum_sq.resize(n);
+        rcnt.resize(n);
+        N2W_CUDA(cudaMemcpyAsync(rsum.data(), r->r_sum, 8 * n, cudaMemcpyDeviceToHost, st));
+        N2W_CUDA(cudaMemcpyAsync(rsum_sq.data(), r->r_sum_sq, 8 * n, cudaMemcpyDeviceToHost, st));
+        N2W_CUDA(cudaMemcpyAsync(rcnt.data(), r->r_count, 4 * n, cudaMemcpyDeviceToHost, st));
+      }
+      N2W_CUDA(cudaStreamSynchronize(st));
+      r->mean.resize(n);
+      r->stderr_.resize(n);
+      for (int64_t p = 0; p < n; ++p) {
+        const double c = cnt[p];
+        double m = c > 0 ? sum[p] / c : 0.0;
+        double ev = mean_variance(sum[p], sum_sq[p], c);
+        if (r->nc) {
+          // NC+2LMC estimate: coarse mean + residual mean, variances add
+          const double rc = rcnt[p];
+          m += rc > 0 ? rsum[p] / rc : 0.0;
+          ev += mean_variance(rsum[p], rsum_sq[p], rc);
+        }
+        r->mean[p] = m;
+        r->stderr_[p] = std::sqrt(ev);
+      }
+      std::lock_guard<std::mutex> lk(s.mu);
+      s.pool->release(r->pool_off, r->pool_len);
+      r->state = reached ? N2W_REQUEST_DONE : N2W_REQUEST_CAPPED;
+      r->t_finish = now_ns();
+      r->h_points.clear();
+      r->h_points.shrink_to_fit();
+      s.active.erase(std::find(s.active.begin(), s.active.end(), r->id));
+      s.stats.completed += 1;
+      s.cv_done.notify_all();
+    } else {
+      // Next sweep: the walks the standard-error model predicts are still
+      // needed (stderr ~ 1/sqrt(N)), plus 10 %, within [32, cap - done].
+      const double need = static_cast<double>(r->walks_done) *
+                              std::pow(static_cast<double>(se) / r->req.target_stderr, 2.0) * 1.1 -
+                          static_cast<double>(r->walks_done);
+      int64_t w = static_cast<int64_t>(std::ceil(std::isfinite(need) ? need : 1e9));
+      w = std::max<int64_t>(w, std::max<int64_t>(32, r->req.min_walks_per_point - r->walks_done));
+      w = std::min<int64_t>(w, r->req.max_walks_per_point - r->walks_done);
+      w = std::min<int64_t>(w, 1 << 20);
+      r->sweep_walks = static_cast<int>(std::max<int64_t>(w, 1));
+      if (r->nc) r->residual_walks = residual_walks_for(r->ncfg, r->sweep_walks);
+    }
   }
 }
 
@@ -276,7 +452,10 @@ void tick(n2w_server& s) {
   std::vector<n2w_server::Request*> act;
   {
     std::lock_guard<std::mutex> lk(s.mu);
-    for (int64_t id : s.active) act.push_back(s.requests.at(id).get());
+    for (int64_t id : s.active) {
+      auto* r = s.requests.at(id).get();
+      if (!r->nc) act.push_back(r);
+    }
   }
   if (act.empty()) return;
   // The tick's walk budget goes to the requests with the least remaining
@@ -363,16 +542,7 @@ void tick(n2w_server& s) {
   if (!swept.empty()) {
     N2W_CUDA(cudaMemsetAsync(s.d_conv, 0, sizeof(unsigned) * swept.size(), st));
     N2W_CUDA(cudaMemsetAsync(s.d_conv_sum, 0, sizeof(double) * swept.size(), st));
-    for (size_t i = 0; i < swept.size(); ++i) {
-      const int64_t n = swept[i]->req.point_count;
-      const int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 1024));
-      stderr_kernel<<<grid, 256, 0, st>>>(swept[i]->sum, swept[i]->sum_sq, swept[i]->count, n, s.d_conv + i,
-                                          s.d_conv_sum + i);
-      N2W_CUDA(cudaGetLastError());
-    }
-    N2W_CUDA(cudaMemcpyAsync(s.h_conv, s.d_conv, sizeof(unsigned) * swept.size(), cudaMemcpyDeviceToHost, st));
-    N2W_CUDA(cudaMemcpyAsync(s.h_conv_sum, s.d_conv_sum, sizeof(double) * swept.size(), cudaMemcpyDeviceToHost,
-                             st));
+    launch_sweep_stderr(s, swept);
   }
   N2W_CUDA(cudaStreamSynchronize(st));
   {
@@ -386,59 +556,98 @@ void tick(n2w_server& s) {
     sl.r->cursor += sl.count;
     sl.r->ticks += 1;
   }
-  // Sweep bookkeeping and completion.
-  for (size_t i = 0; i < swept.size(); ++i) {
-    auto* r = swept[i];
-    float mx;
-    std::memcpy(&mx, &s.h_conv[i], sizeof(float));
-    r->max_stderr = mx;
-    r->rms_stderr = static_cast<float>(std::sqrt(s.h_conv_sum[i] / static_cast<double>(r->req.point_count)));
-    // the norm the request asked for drives both stopping and the next sweep's size
-    const float se = r->req.stderr_norm == N2W_STDERR_RMS ? r->rms_stderr : r->max_stderr;
-    r->walks_done += r->sweep_walks;
-    r->cursor = 0;
-    r->sweep += 1;
-    const bool reached = se <= r->req.target_stderr && r->walks_done >= r->req.min_walks_per_point;
-    const bool capped = r->walks_done >= r->req.max_walks_per_point;
-    if (reached || capped) {
-      const int64_t n = r->req.point_count;
-      std::vector<double> sum(n), sum_sq(n);
-      std::vector<uint32_t> cnt(n);
-      N2W_CUDA(cudaMemcpyAsync(sum.data(), r->sum, 8 * n, cudaMemcpyDeviceToHost, st));
-      N2W_CUDA(cudaMemcpyAsync(sum_sq.data(), r->sum_sq, 8 * n, cudaMemcpyDeviceToHost, st));
-      N2W_CUDA(cudaMemcpyAsync(cnt.data(), r->count, 4 * n, cudaMemcpyDeviceToHost, st));
-      N2W_CUDA(cudaStreamSynchronize(st));
-      r->mean.resize(n);
-      r->stderr_.resize(n);
-      for (int64_t p = 0; p < n; ++p) {
-        const double c = cnt[p];
-        const double m = c > 0 ? sum[p] / c : 0.0;
-        const double v = c > 1 ? std::max(0.0, (sum_sq[p] - c * m * m) / (c - 1.0)) : 0.0;
-        r->mean[p] = m;
-        r->stderr_[p] = c > 0 ? std::sqrt(v / c) : INFINITY;
-      }
-      std::lock_guard<std::mutex> lk(s.mu);
-      s.pool->release(r->pool_off, r->pool_len);
-      r->state = reached ? N2W_REQUEST_DONE : N2W_REQUEST_CAPPED;
-      r->t_finish = now_ns();
-      r->h_points.clear();
-      r->h_points.shrink_to_fit();
-      s.active.erase(std::find(s.active.begin(), s.active.end(), r->id));
-      s.stats.completed += 1;
-      s.cv_done.notify_all();
-    } else {
-      // Next sweep: the walks the standard-error model predicts are still
-      // needed (stderr ~ 1/sqrt(N)), plus 10 %, within [32, cap - done].
-      const double need = static_cast<double>(r->walks_done) *
-                              std::pow(static_cast<double>(se) / r->req.target_stderr, 2.0) * 1.1 -
-                          static_cast<double>(r->walks_done);
-      int64_t w = static_cast<int64_t>(std::ceil(std::isfinite(need) ? need : 1e9));
-      w = std::max<int64_t>(w, std::max<int64_t>(32, r->req.min_walks_per_point - r->walks_done));
-      w = std::min<int64_t>(w, r->req.max_walks_per_point - r->walks_done);
-      w = std::min<int64_t>(w, 1 << 20);
-      r->sweep_walks = static_cast<int>(std::max<int64_t>(w, 1));
+  finish_sweeps(s, swept);
+}
+
+// NC+2LMC work between two ticks: chunks of kNcChunk points, shortest
+// remaining sweep first, until tick_walks coarse + residual walks have run
+// (at least one chunk).  Each chunk is keyed by (request seed, sweep, chunk
+// index) alone.
+void nc_step(n2w_server& s) {
+  std::vector<n2w_server::Request*> act;
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    for (int64_t id : s.active) {
+      auto* r = s.requests.at(id).get();
+      if (r->nc) act.push_back(r);
     }
   }
+  if (act.empty()) return;
+  auto remaining = [](const n2w_server::Request* r) {
+    return (r->req.point_count - r->cursor) * static_cast<int64_t>(r->sweep_walks + r->residual_walks);
+  };
+  std::stable_sort(act.begin(), act.end(),
+                   [&](const n2w_server::Request* a, const n2w_server::Request* b) { return remaining(a) < remaining(b); });
+  const cudaStream_t st = s.stream;
+  double* c_sum = reinterpret_cast<double*>(s.d_nc_scratch);
+  double* c_sum_sq = c_sum + kNcChunk;
+  double* r_sum = c_sum_sq + kNcChunk;
+  double* r_sum_sq = r_sum + kNcChunk;
+  uint64_t* c_steps = reinterpret_cast<uint64_t*>(r_sum_sq + kNcChunk);
+  uint32_t* c_count = reinterpret_cast<uint32_t*>(c_steps + kNcChunk);
+  uint32_t* c_forced = c_count + kNcChunk;
+  uint32_t* r_count = c_forced + kNcChunk;
+  int64_t left = s.opt.tick_walks, chunks = 0, walks = 0;
+  std::vector<n2w_server::Request*> swept;
+  for (auto* r : act) {
+    if (left <= 0) break;
+    while (left > 0 && r->cursor < r->req.point_count) {
+      const int64_t first = r->cursor;
+      const int64_t np = std::min(kNcChunk, r->req.point_count - first);
+      n2w_nc2lmc_options o{};
+      o.coarse_walks = r->sweep_walks;
+      o.residual_walks = r->residual_walks;
+      o.depth_m = r->ncfg.depth_m;
+      o.max_steps = s.opt.max_steps;
+      o.epsilon = s.opt.epsilon;
+      o.step_scale = s.opt.step_scale;
+      o.seed = splitmix64(r->req.seed ^ splitmix64((static_cast<uint64_t>(r->sweep) << 40) +
+                                                   static_cast<uint64_t>(first / kNcChunk)));
+      for (int k = 0; k < 3; ++k) {
+        o.input_min[k] = r->ncfg.input_min[k];
+        o.input_extent[k] = r->ncfg.input_extent[k];
+      }
+      n2w_point_stats co{c_sum, c_sum_sq, c_count, c_steps, c_forced};
+      n2w_point_stats re{r_sum, r_sum_sq, r_count, nullptr, nullptr};
+      const int rc = n2w_nc2lmc_estimate_ex(s.bvhs[r->req.mesh], &s.problems[r->req.problem], r->ncfg.cache,
+                                            r->d_points + first, np, &o, co, re, nullptr, st);
+      if (rc != N2W_OK) throw Error(rc, n2w_last_error());
+      NcChunkAdd add;
+      add.c_sum = c_sum;
+      add.c_sum_sq = c_sum_sq;
+      add.r_sum = r_sum;
+      add.r_sum_sq = r_sum_sq;
+      add.c_count = c_count;
+      add.c_forced = c_forced;
+      add.r_count = r_count;
+      add.c_steps = c_steps;
+      add.t_c_sum = r->sum + first;
+      add.t_c_sum_sq = r->sum_sq + first;
+      add.t_r_sum = r->r_sum + first;
+      add.t_r_sum_sq = r->r_sum_sq + first;
+      add.t_c_count = r->count + first;
+      add.t_c_forced = r->forced + first;
+      add.t_r_count = r->r_count + first;
+      add.t_c_steps = r->steps + first;
+      add_nc_chunk_kernel<<<static_cast<int>((np + 255) / 256), 256, 0, st>>>(add, np);
+      N2W_CUDA(cudaGetLastError());
+      const int64_t w = np * static_cast<int64_t>(r->sweep_walks + r->residual_walks);
+      left -= w;
+      walks += w;
+      chunks += 1;
+      r->cursor += np;
+      r->ticks += 1;
+    }
+    if (r->cursor == r->req.point_count) swept.push_back(r);
+  }
+  if (!swept.empty()) launch_sweep_stderr(s, swept);
+  N2W_CUDA(cudaStreamSynchronize(st));
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.stats.nc_chunks += chunks;
+    s.stats.nc_walks += walks;
+  }
+  finish_sweeps(s, swept);
 }
 
 void worker_loop(n2w_server* s) {
@@ -452,6 +661,7 @@ void worker_loop(n2w_server* s) {
     try {
       admit(*s);
       tick(*s);
+      nc_step(*s);
     } catch (const std::exception& e) {
       std::lock_guard<std::mutex> lk(s->mu);
       fail_all_locked(*s, std::string("serving loop stopped: ") + e.what());
@@ -487,6 +697,7 @@ void destroy_server(n2w_server* s) {
   cudaFreeHost(s->h_insts);
   cudaFreeHost(s->h_conv);
   cudaFree(s->d_conv_sum);
+  cudaFree(s->d_nc_scratch);
   cudaFreeHost(s->h_conv_sum);
   cudaFreeHost(s->h_counters);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -538,6 +749,7 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     const int rc = n2w_scene_create(bvhs, mesh_count, &sc);
     if (rc != N2W_OK) throw Error(rc, n2w_last_error());
     s->scene.reset(sc);
+    s->bvhs.assign(bvhs, bvhs + mesh_count);
     s->problems.assign(problems, problems + problem_count);
     N2W_CUDA(cudaMalloc(&s->d_problems, sizeof(n2w_problem) * problem_count));
     N2W_CUDA(cudaMemcpy(s->d_problems, problems, sizeof(n2w_problem) * problem_count, cudaMemcpyHostToDevice));
@@ -566,12 +778,27 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     N2W_CUDA(cudaMalloc(&s->d_conv_sum, sizeof(double) * o.max_inflight));
     N2W_CUDA(cudaMallocHost(&s->h_conv_sum, sizeof(double) * o.max_inflight));
     N2W_CUDA(cudaMallocHost(&s->h_counters, sizeof(n2w_walk_counters)));
+    // coarse sum, sum_sq, residual sum, sum_sq, coarse steps (8 B); coarse count, forced, residual count (4 B)
+    N2W_CUDA(cudaMalloc(&s->d_nc_scratch, kNcChunk * (5 * 8 + 3 * 4)));
     N2W_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->worker = std::thread(worker_loop, s);
     *out = s;
   });
   if (st != N2W_OK && s) destroy_server(s);
   return st;
+}
+
+int n2w_server_set_nc(n2w_server* s, int mesh, int problem, const n2w_server_nc* nc) {
+  return guarded([&] {
+    N2W_REQUIRE(s && nc, "n2w_server_set_nc: null argument");
+    N2W_REQUIRE(mesh >= 0 && mesh < static_cast<int>(s->bvhs.size()), "mesh index out of range");
+    N2W_REQUIRE(problem >= 0 && problem < static_cast<int>(s->problems.size()), "problem index out of range");
+    N2W_REQUIRE(nc->depth_m >= 0, "depth_m must be >= 0");
+    N2W_REQUIRE(nc->residual_fraction > 0.0f && nc->residual_fraction <= 1.0f, "residual_fraction must be in (0, 1]");
+    for (int k = 0; k < 3; ++k) N2W_REQUIRE(nc->input_extent[k] > 0.0f, "input_extent must be positive");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->nc[{mesh, problem}] = *nc;
+  });
 }
 
 int n2w_server_submit(n2w_server* s, const n2w_request* req, const float* h_points, int64_t* id_out) {
@@ -586,17 +813,25 @@ int n2w_server_submit(n2w_server* s, const n2w_request* req, const float* h_poin
     N2W_REQUIRE(req->max_walks_per_point >= 1 && req->min_walks_per_point >= 0 &&
                     req->min_walks_per_point <= req->max_walks_per_point,
                 "need 0 <= min_walks_per_point <= max_walks_per_point, max >= 1");
-    if (request_bytes(req->point_count) > s->pool->capacity()) {
+    N2W_REQUIRE(req->mode == N2W_REQUEST_MODE_PLAIN || req->mode == N2W_REQUEST_MODE_NC2LMC, "bad request mode");
+    const bool nc = req->mode == N2W_REQUEST_MODE_NC2LMC;
+    if (request_bytes(req->point_count, nc) > s->pool->capacity()) {
       throw Error(N2W_ENOMEM, "request of " + std::to_string(req->point_count) +
                                   " points needs more device memory than the whole serving pool (" +
                                   std::to_string(s->pool->capacity()) + " bytes)");
     }
     auto r = std::make_unique<n2w_server::Request>();
     r->req = *req;
+    r->nc = nc;
     r->h_points.assign(h_points, h_points + 3 * req->point_count);
     r->t_submit = now_ns();
     std::lock_guard<std::mutex> lk(s->mu);
     if (!s->fatal.empty()) throw Error(N2W_ECUDA, s->fatal);
+    if (nc) {
+      auto it = s->nc.find({req->mesh, req->problem});
+      N2W_REQUIRE(it != s->nc.end(), "NC+2LMC request: no cache registered for this (mesh, problem)");
+      r->ncfg = it->second;
+    }
     r->id = s->next_id++;
     *id_out = r->id;
     s->pending.push_back(r->id);
@@ -642,6 +877,7 @@ int n2w_server_wait(n2w_server* s, int64_t id, double timeout_seconds, double* h
       info->rms_stderr = r->rms_stderr;
       info->queue_seconds = (r->t_admit ? r->t_admit - r->t_submit : 0) * 1e-9;
       info->latency_seconds = (r->t_finish - r->t_submit) * 1e-9;
+      info->residual_walks_per_point = r->residual_done;
     }
     if (r->state == N2W_REQUEST_FAILED) {
       const std::string msg = r->error;

@@ -574,7 +574,9 @@ class Server:
     """Continuous-batching WoS server (native worker thread; see n2w_server_*).
 
     meshes: list of Bvh; problems: list of Problem.  submit() returns a request
-    id; wait() returns (mean, stderr, info dict)."""
+    id; wait() returns (mean, stderr, info dict).  set_nc() registers a
+    pre-trained Cache for NC+2LMC requests (submit(..., mode="nc2lmc")); the
+    server keeps references to the BVHs and caches it walks."""
 
     def __init__(self, bvhs, problems, **options):
         from ._lib import ServerOptions
@@ -590,15 +592,37 @@ class Server:
         call("n2w_server_create", arr, len(bvhs), self._problems, len(problems), C.byref(o), C.byref(h))
         self._h = h
         self._sizes = {}
+        self._bvhs = list(bvhs)
+        self._caches = {}
+
+    def set_nc(self, mesh: int, problem: int, cache, input_min, input_extent, depth_m: int = 8,
+               residual_fraction: float = 1.0 / 16):
+        """Cache for NC+2LMC requests on (mesh, problem); cache=None selects the
+        analytic cache C(x) = u(x) (a check of the estimator)."""
+        from ._lib import ServerNc
+
+        c = ServerNc()
+        c.cache = cache.handle if cache is not None else None
+        c.input_min[:] = [float(v) for v in input_min]
+        c.input_extent[:] = [float(v) for v in input_extent]
+        c.depth_m = depth_m
+        c.residual_fraction = residual_fraction
+        call("n2w_server_set_nc", self._h, mesh, problem, C.byref(c))
+        self._caches[(mesh, problem)] = cache
 
     def submit(self, mesh: int, problem: int, points: np.ndarray, target_stderr: float, seed: int = 1,
-               min_walks: int = 32, max_walks: int = 1 << 16, rms: bool = False) -> int:
+               min_walks: int = 32, max_walks: int = 1 << 16, rms: bool = False, mode: str = "plain") -> int:
         """rms=False: every point meets the target; rms=True: the root mean
-        square of the per-point standard errors does."""
-        from ._lib import Request
+        square of the per-point standard errors does.  mode: "plain" WoS or
+        "nc2lmc" with the cache set_nc registered (max/min walks count the
+        coarse walks)."""
+        from ._lib import N2W_REQUEST_MODE_NC2LMC, N2W_REQUEST_MODE_PLAIN, Request
 
+        modes = {"plain": N2W_REQUEST_MODE_PLAIN, "nc2lmc": N2W_REQUEST_MODE_NC2LMC}
+        if mode not in modes:
+            raise ValueError(f"mode must be one of {sorted(modes)}")
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
-        r = Request(mesh, problem, len(pts), target_stderr, min_walks, max_walks, seed, 1 if rms else 0, 0)
+        r = Request(mesh, problem, len(pts), target_stderr, min_walks, max_walks, seed, 1 if rms else 0, modes[mode])
         rid = C.c_int64()
         call("n2w_server_submit", self._h, C.byref(r), _ptr(pts), C.byref(rid))
         self._sizes[rid.value] = len(pts)

@@ -132,22 +132,28 @@ class Request(C.Structure):
     _fields_ = [("mesh", C.c_int32), ("problem", C.c_int32), ("point_count", C.c_int64),
                 ("target_stderr", C.c_float), ("min_walks_per_point", C.c_int32),
                 ("max_walks_per_point", C.c_int32), ("seed", C.c_uint64), ("stderr_norm", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("mode", C.c_int32)]
+
+
+class ServerNc(C.Structure):
+    _fields_ = [("cache", C.c_void_p), ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3),
+                ("depth_m", C.c_int32), ("residual_fraction", C.c_float)]
 
 
 class RequestInfo(C.Structure):
     _fields_ = [("state", C.c_int32), ("sweeps", C.c_int32), ("walks_per_point", C.c_int64), ("ticks", C.c_int64),
                 ("max_stderr", C.c_float), ("rms_stderr", C.c_float), ("queue_seconds", C.c_double),
-                ("latency_seconds", C.c_double)]
+                ("latency_seconds", C.c_double), ("residual_walks_per_point", C.c_int64)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in
                 ("submitted", "completed", "inflight", "pending", "peak_inflight", "ticks", "walks", "walk_steps",
-                 "overflow", "pool_bytes", "pool_used", "peak_pool_bytes")]
+                 "overflow", "pool_bytes", "pool_used", "peak_pool_bytes", "nc_chunks", "nc_walks")]
 
 
 N2W_REQUEST_PENDING, N2W_REQUEST_ACTIVE, N2W_REQUEST_DONE, N2W_REQUEST_CAPPED, N2W_REQUEST_FAILED = range(5)
+N2W_REQUEST_MODE_PLAIN, N2W_REQUEST_MODE_NC2LMC = 0, 1
 N2W_LABEL_EXACT, N2W_LABEL_WOS = 0, 1
 N2W_SLICE_RULE_RENDER, N2W_SLICE_RULE_EVAL = 0, 1
 
@@ -248,6 +254,7 @@ _SIGS = {
     "n2w_batch_destroy": (None, [P]),
     "n2w_server_options_default": (I, [C.POINTER(ServerOptions)]),
     "n2w_server_create": (I, [C.POINTER(C.c_void_p), I, C.POINTER(Problem), I, C.POINTER(ServerOptions), PP]),
+    "n2w_server_set_nc": (I, [P, I, I, C.POINTER(ServerNc)]),
     "n2w_server_submit": (I, [P, C.POINTER(Request), P, C.POINTER(I64)]),
     "n2w_server_poll": (I, [P, I64, C.POINTER(I)]),
     "n2w_server_wait": (I, [P, I64, C.c_double, P, P, C.POINTER(RequestInfo)]),

@@ -4,7 +4,9 @@ Checks that a request gives the same answer alone and in a mix (same walk
 counts, FP64 sums equal to rounding of the addition order), that results meet
 their target standard error against the FP64 analytic solution, that admission
 respects the device pool (oversized requests refused, the rest queued until
-memory frees), that concurrent requests share launches, and the walk cap.
+memory frees), that concurrent requests share launches, and the walk cap;
+NC+2LMC requests (a trained cache, and the analytic cache) are unbiased and
+also the same alone and in a mix of plain and NC+2LMC requests.
 """
 import numpy as np
 import pytest
@@ -103,4 +105,42 @@ def test_small_requests_share_launches_and_walk_cap(gpu, meshes):
     rid = srv.submit(1, 0, p[:5], 1e-6, seed=3, min_walks=32, max_walks=96)
     _, se, info = srv.wait(rid, timeout=120)
     assert info["state"] == 3 and info["walks_per_point"] == 96  # N2W_REQUEST_CAPPED
+    srv.close()
+
+
+def test_nc2lmc_requests_alone_equal_mix_and_unbiased(gpu, meshes):
+    from n2w import nc
+
+    probs = problems(gpu)
+    bvhs = [b for _, b in meshes]
+    m0, m1 = meshes[0][0], meshes[1][0]
+    cache = gpu.Cache(gpu.cache_config(log2_hashmap_size=16, max_resolution=256.0))
+    nc.train(cache, bvhs[0], probs[0], m0, steps=60, batch=8192, walks_per_label=32, epsilon=1e-3)
+    srv = gpu.Server(bvhs, probs, pool_bytes=64 << 20, tick_walks=1 << 17, epsilon=1e-3)
+    srv.set_nc(0, 0, cache, *nc.input_box(m0), depth_m=4, residual_fraction=0.25)
+    srv.set_nc(1, 1, None, *nc.input_box(m1), depth_m=2, residual_fraction=0.5)
+    with pytest.raises(gpu.N2wError, match="no cache registered"):
+        srv.submit(1, 0, points(meshes, 1, 4, seed=2), 1e-2, mode="nc2lmc")
+    pa = points(meshes, 0, 5000, seed=21)  # two chunks of the NC path
+    ra = srv.submit(0, 0, pa, 3e-2, seed=5, mode="nc2lmc")
+    mean_a, se_a, info_a = srv.wait(ra, timeout=300)
+    check_accuracy(gpu, probs[0], pa, mean_a, se_a, info_a, 3e-2)
+    assert info_a["residual_walks_per_point"] >= max(2, info_a["walks_per_point"] // 4)
+    assert info_a["ticks"] >= 2 * info_a["sweeps"]
+    mix = []
+    for k, (mesh, prob, n, tgt, mode) in enumerate([(1, 1, 3000, 2e-2, "nc2lmc"), (0, 0, 800, 2e-2, "plain"),
+                                                    (1, 1, 50, 1e-2, "plain"), (0, 0, 9, 1e-2, "nc2lmc")]):
+        p = points(meshes, mesh, n, seed=40 + k)
+        mix.append((srv.submit(mesh, prob, p, tgt, seed=60 + k, mode=mode), prob, p, tgt))
+    rb = srv.submit(0, 0, pa, 3e-2, seed=5, mode="nc2lmc")
+    mean_b, se_b, info_b = srv.wait(rb, timeout=300)
+    assert info_b["walks_per_point"] == info_a["walks_per_point"]
+    assert info_b["residual_walks_per_point"] == info_a["residual_walks_per_point"]
+    np.testing.assert_allclose(mean_b, mean_a, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(se_b, se_a, rtol=1e-9, atol=1e-14)
+    for rid, prob, p, tgt in mix:
+        m, s, info = srv.wait(rid, timeout=300)
+        check_accuracy(gpu, probs[prob], p, m, s, info, tgt)
+    st = srv.stats()
+    assert st["completed"] == 6 and st["nc_chunks"] >= 6 and st["nc_walks"] > 0 and st["pool_used"] == 0
     srv.close()

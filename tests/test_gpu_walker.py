@@ -230,10 +230,11 @@ def test_invalid_options(gpu, small_scene):
                {"block_size": 48}, {"block_size": 512}):
         with pytest.raises(gpu.N2wError):
             run(gpu, bvh, p, pts, **kw)
-    bad = gpu.problem_charges_seeded()
-    bad.mode = 13
-    with pytest.raises(gpu.N2wError):
-        run(gpu, bvh, bad, pts)
+    for mode in (17, 29, 33, 99, 102):  # outside the modes 0-16, 30-32, 100-101
+        bad = gpu.problem_charges_seeded()
+        bad.mode = mode
+        with pytest.raises(gpu.N2wError):
+            run(gpu, bvh, bad, pts)
     r, cnt = run(gpu, bvh, p, pts[:0])
     assert len(r["mean"]) == 0
 
