@@ -434,14 +434,17 @@ def run_serve(args):
     boundary or the config-1 manufactured Poisson problem; points uniform in
     the interior (ball r = 0.9 masked by the mesh); a fraction of large
     requests.  Each request stops when the root mean square of its per-point
-    standard errors meets its target.  Latency is measured natively
+    standard errors meets its target.  A fraction (--serve-nc-fraction) of the
+    requests are NC+2LMC requests on the icosphere with the Poisson problem,
+    served with a cache trained online before the timed region (depth 1,
+    residual walks = 1/2 of the coarse walks).  Latency is measured natively
     (submission -> result ready).  The run stops at --serve-time-limit and
     then reports how many requests had not finished."""
     import threading as th
 
     import n2w
     from n2w import workloads
-    from n2w._lib import N2W_ETIMEOUT, call
+    from n2w._lib import N2W_REQUEST_DONE, call
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     call("n2w_set_device", local)
@@ -454,6 +457,17 @@ def run_serve(args):
     problems = [n2w.problem_charges_seeded(8, 1.6, 2.0, seed=2024), n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)]
     problems[1].source_samples = args.serve_source_samples  # variance reduction of the Poisson source term
     srv = n2w.Server(bvhs, problems, tick_walks=args.serve_tick_walks, epsilon=1e-3)
+    nc_train = None
+    if args.serve_nc_fraction > 0:
+        from n2w import nc
+
+        cache = n2w.Cache(n2w.cache_config())
+        tt = time.perf_counter()
+        losses = nc.train(cache, bvhs[1], problems[1], meshes[1], steps=args.serve_nc_train_steps, batch=65536,
+                          walks_per_label=32, epsilon=1e-3)
+        nc_train = {"seconds": time.perf_counter() - tt, "steps": args.serve_nc_train_steps, "batch": 65536,
+                    "walks_per_label": 32, "loss_first_last": [float(losses[0]), float(losses[-1])]}
+        srv.set_nc(1, 1, cache, *nc.input_box(meshes[1]), depth_m=1, residual_fraction=0.5)
     N = args.serve_requests
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, N))
     reqs = []
@@ -463,10 +477,13 @@ def run_serve(args):
         n = min(workloads.log_uniform_int(rng, lo, hi), 65536)
         mesh = int(rng.integers(0, 4))
         prob = int(rng.uniform() < args.serve_poisson_fraction)
+        mode = "nc2lmc" if rng.uniform() < args.serve_nc_fraction else "plain"
+        if mode == "nc2lmc":
+            mesh, prob = 1, 1
         tgt = 1e-3 if (prob == 0 and n <= 256 and rng.uniform() < 0.5) else 1e-2
         off = int(rng.integers(0, 65536 - n + 1))
         reqs.append({"t": float(arrivals[k]), "n": n, "mesh": mesh, "problem": prob, "target": tgt, "off": off,
-                     "seed": int(rng.integers(1, 2**62))})
+                     "seed": int(rng.integers(1, 2**62)), "mode": mode})
     ids = [None] * N
     stop = th.Event()
     errors = []
@@ -484,7 +501,7 @@ def run_serve(args):
                     return
                 pts = pool_pts[r["mesh"]][r["off"]:r["off"] + r["n"]]
                 ids[k] = srv.submit(r["mesh"], r["problem"], pts, r["target"], seed=r["seed"],
-                                    max_walks=args.serve_max_walks, rms=True)
+                                    max_walks=args.serve_max_walks, rms=True, mode=r["mode"])
         except Exception as e:  # surfaced by the collector below
             errors.append(e)
             stop.set()
@@ -493,35 +510,40 @@ def run_serve(args):
     deadline = t0 + args.serve_time_limit
     results = []
     last = t0
+    outstanding = {}  # request index -> id, submitted and not yet collected
+    next_k = 0
     with ClockSampler(local) as clocks:
         sub.start()
-        k = 0
-        while k < N and not errors:
+        while len(results) < N and not errors:
             now = time.perf_counter()
             if now > deadline:
                 break
             if now - last > 5.0:
                 st = srv.stats()
-                print(f"[serve] t={now - t0:.0f}s done={k}/{N} submitted={st['submitted']} "
+                print(f"[serve] t={now - t0:.0f}s done={len(results)}/{N} submitted={st['submitted']} "
                       f"inflight={st['inflight']} pending={st['pending']} ticks={st['ticks']} "
-                      f"walk_steps={st['walk_steps']:.3g}", file=sys.stderr, flush=True)
+                      f"nc_chunks={st['nc_chunks']} walk_steps={st['walk_steps']:.3g}", file=sys.stderr, flush=True)
                 last = now
-            if ids[k] is None:
-                time.sleep(0.001)
-                continue
-            try:
-                mean, se, info = srv.wait(ids[k], timeout=min(1.0, max(0.01, deadline - now)))
-            except n2w.N2wError as e:
-                if e.code == N2W_ETIMEOUT:
+            while next_k < N and ids[next_k] is not None:
+                outstanding[next_k] = ids[next_k]
+                next_k += 1
+            collected = False
+            # requests finish out of order; latency is the server's own timestamp, so
+            # collecting order does not affect it
+            for k, rid in list(outstanding.items()):
+                if srv.poll(rid) < N2W_REQUEST_DONE:
                     continue
-                raise
-            r = reqs[k]
-            pts = pool_pts[r["mesh"]][r["off"]:r["off"] + r["n"]]
-            exact = n2w.problem_exact(problems[r["problem"]], pts.astype(np.float64))
-            results.append({"n": r["n"], "latency": info["latency_seconds"], "queue": info["queue_seconds"],
-                            "mse": float(np.mean((mean - exact) ** 2)), "target": r["target"],
-                            "state": info["state"], "walks": info["walks_per_point"]})
-            k += 1
+                mean, se, info = srv.wait(rid, timeout=0.0)
+                del outstanding[k]
+                collected = True
+                r = reqs[k]
+                pts = pool_pts[r["mesh"]][r["off"]:r["off"] + r["n"]]
+                exact = n2w.problem_exact(problems[r["problem"]], pts.astype(np.float64))
+                results.append({"n": r["n"], "latency": info["latency_seconds"], "queue": info["queue_seconds"],
+                                "mse": float(np.mean((mean - exact) ** 2)), "target": r["target"],
+                                "state": info["state"], "walks": info["walks_per_point"], "mode": r["mode"]})
+            if not collected:
+                time.sleep(0.002)
         stop.set()
         makespan = time.perf_counter() - t0
     if errors:
@@ -534,6 +556,15 @@ def run_serve(args):
     small = np.array([r["latency"] for r in results if r["n"] <= 4096]) if results else np.array([np.nan])
     mse_ratio = np.array([r["mse"] / r["target"] ** 2 for r in results]) if results else np.array([np.nan])
     complete = done == N
+
+    def by_mode(mode):
+        rs = [r for r in results if r["mode"] == mode]
+        if not rs:
+            return {"finished": 0}
+        lat_m = np.array([r["latency"] for r in rs])
+        ratio = np.array([r["mse"] / r["target"] ** 2 for r in rs])
+        return {"finished": len(rs), "p50_s": float(np.percentile(lat_m, 50)), "p99_s": float(np.percentile(lat_m, 99)),
+                "median_mse_over_target2": float(np.median(ratio)), "points": int(sum(r["n"] for r in rs))}
     line = {
         "metric": "p99 latency of <=4096-point requests, serving loop under mixed load (s)",
         "value": float(np.percentile(small, 99)) if complete else None, "unit": "s", "n_gpus": 1, "steps": N,
@@ -545,7 +576,8 @@ def run_serve(args):
                                f"{args.serve_source_samples} source samples per ball), points "
                                f"log-uniform 1..4096 ({100 * args.serve_large_fraction:.0f}% log-uniform "
                                f"4096..{args.serve_large_max}), RMS stderr target 1e-2 (1e-3 for half of the "
-                               "<=256-point harmonic requests)",
+                               f"<=256-point harmonic requests); {100 * args.serve_nc_fraction:.0f}% NC+2LMC "
+                               "requests (icosphere, Poisson problem, pre-trained cache, m = 1, residual 1/2)",
                    "tick_walks": args.serve_tick_walks, "max_walks_per_point": args.serve_max_walks,
                    "seed": args.serve_seed, "time_limit_s": args.serve_time_limit},
         "complete": complete, "finished_requests": done,
@@ -558,8 +590,11 @@ def run_serve(args):
                      "p99_mse_over_target2": float(np.percentile(mse_ratio, 99)),
                      "done": int(sum(r["state"] == 2 for r in results)),
                      "capped": int(sum(r["state"] == 3 for r in results))},
+        "modes": {"plain": by_mode("plain"), "nc2lmc": by_mode("nc2lmc")}, "nc_cache_training": nc_train,
         "server": st, "clocks": clocks.summary(),
-        "gpu_launches": int(st["ticks"]) * 2,
+        # plain ticks: first query + walker; NC+2LMC chunks: per level first query, walker, cache
+        # inference, combine and reduction, plus the chunk's add (more when a chunk splits into batches)
+        "gpu_launches": int(st["ticks"]) * 2 + int(st["nc_chunks"]) * 11,
     }
     print(json.dumps(line))
     return 0
@@ -580,8 +615,8 @@ def main():
     ap.add_argument("--workload", default="slice", choices=["slice", "batch", "serve"],
                     help="slice: the headline Poisson slice (default); batch: 64 batched Laplace instances; "
                          "serve: the serving loop under Poisson arrivals")
-    ap.add_argument("--serve-requests", type=int, default=600)
-    ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-rate", type=float, default=10.0, help="mean arrivals per second")
     ap.add_argument("--serve-large-fraction", type=float, default=0.05)
     ap.add_argument("--serve-large-max", type=int, default=16384)
     ap.add_argument("--serve-poisson-fraction", type=float, default=0.25)
@@ -591,6 +626,9 @@ def main():
                     help="Green's-function source samples per ball of the Poisson problem")
     ap.add_argument("--serve-tick-walks", type=int, default=1 << 21)
     ap.add_argument("--serve-seed", type=int, default=4242)
+    ap.add_argument("--serve-nc-fraction", type=float, default=0.1,
+                    help="fraction of requests served as NC+2LMC with a pre-trained cache")
+    ap.add_argument("--serve-nc-train-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

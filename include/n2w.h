@@ -644,6 +644,7 @@ typedef struct n2w_server_stats {
   int64_t ticks, walks, walk_steps, overflow;
   int64_t pool_bytes, pool_used, peak_pool_bytes;
   int64_t nc_chunks, nc_walks; /* NC+2LMC chunks run and their coarse + residual walks */
+  int64_t tick_us, nc_us;      /* worker wall time in plain ticks / NC+2LMC steps (incl. syncs) */
 } n2w_server_stats;
 
 typedef struct n2w_server n2w_server;

@@ -160,8 +160,10 @@ size_t request_bytes(int64_t n, bool nc) {
   return static_cast<size_t>(n) * (nc ? 64 : 44) + (nc ? 8 : 5) * 256;
 }
 
-// Points per NC+2LMC chunk (the unit of work and of walk keying).
-constexpr int64_t kNcChunk = 4096;
+// Points per NC+2LMC chunk (the unit of work and of walk keying).  Small
+// enough that one chunk (1,024 points x a few thousand walks) stays within
+// a few tens of milliseconds, so NC work interleaves with the plain ticks.
+constexpr int64_t kNcChunk = 1024;
 
 uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -660,8 +662,14 @@ void worker_loop(n2w_server* s) {
     }
     try {
       admit(*s);
+      const int64_t t0 = now_ns();
       tick(*s);
+      const int64_t t1 = now_ns();
       nc_step(*s);
+      const int64_t t2 = now_ns();
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stats.tick_us += (t1 - t0) / 1000;
+      s->stats.nc_us += (t2 - t1) / 1000;
     } catch (const std::exception& e) {
       std::lock_guard<std::mutex> lk(s->mu);
       fail_all_locked(*s, std::string("serving loop stopped: ") + e.what());

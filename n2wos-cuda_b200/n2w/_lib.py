@@ -149,7 +149,8 @@ class RequestInfo(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in
                 ("submitted", "completed", "inflight", "pending", "peak_inflight", "ticks", "walks", "walk_steps",
-                 "overflow", "pool_bytes", "pool_used", "peak_pool_bytes", "nc_chunks", "nc_walks")]
+                 "overflow", "pool_bytes", "pool_used", "peak_pool_bytes", "nc_chunks", "nc_walks",
+                 "tick_us", "nc_us")]
 
 
 N2W_REQUEST_PENDING, N2W_REQUEST_ACTIVE, N2W_REQUEST_DONE, N2W_REQUEST_CAPPED, N2W_REQUEST_FAILED = range(5)
