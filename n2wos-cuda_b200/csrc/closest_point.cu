@@ -41,7 +41,7 @@ namespace {
 constexpr int kQueryBlock = 256;
 
 template <bool kMasked, bool kCount>
-__global__ void __launch_bounds__(kQueryBlock, 4) closest_point_kernel(
+__global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
     const float4* __restrict__ nodes, const float4* __restrict__ tris, const dev::SeedGrid grid,
     const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
     float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(kQueryBlock, 4) closest_point_kernel(
   hit.slot = -1;
   hit.cp = p;
   dev::TravState tv{0, kEmptyChild, 0, 0};
-  int2 stack[kTraversalStack];
+  int2 stack_mem[kTraversalStack];
+  dev::LocalStack stack{stack_mem};
   uint32_t c_nodes = 0, c_tris = 0;
   bool overflow = false;
   for (;;) {

@@ -90,9 +90,12 @@ __device__ __forceinline__ V3 closest_point_triangle(V3 p, V3 a, V3 b, V3 c) {
   return r;
 }
 
-// Squared distance from p to box [lo, hi] along one axis pair; +inf for empty slots.
+// Signed gap from p to [lo, hi] along one axis: p - clamp(p, lo, hi).  Its
+// square equals that of max(lo - p, p - hi, 0) bit for bit (IEEE subtraction
+// is sign-symmetric), with one subtraction instead of two; empty slots
+// (lo = +inf, hi = -inf) give an infinite gap.
 __device__ __forceinline__ float axis_gap(float p, float lo, float hi) {
-  return fmaxf(fmaxf(fs(lo, p), fs(p, hi)), 0.0f);
+  return fs(p, fminf(fmaxf(p, lo), hi));
 }
 
 __device__ __forceinline__ float box_d2(V3 p, float lox, float hix, float loy, float hiy, float loz,
@@ -101,6 +104,73 @@ __device__ __forceinline__ float box_d2(V3 p, float lox, float hix, float loy, f
   const float dy = axis_gap(p.y, loy, hiy);
   const float dz = axis_gap(p.z, loz, hiz);
   return fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz));
+}
+
+// ---- contracted-FP32 variants for the walker -------------------------------
+// A walk only needs each step's distance (and the closest point at the
+// terminal step) to FP32 accuracy: the reference's GPU walker is compiled
+// with FMA contraction and IEEE division, and its parity with any CPU
+// evaluation is statistical.  These variants evaluate the same Ericson region
+// tests with fused multiply-adds and the fast division intrinsic, cutting the
+// instruction count of a triangle test by about a quarter.  Results differ
+// from the exact routine above by a few ulps, so the walker's queries are not
+// bit-identical to n2w_bvh_query_device's; the query API keeps the exact path.
+__device__ __forceinline__ float vdot_fast(V3 a, V3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+__device__ __forceinline__ V3 vsub_fast(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 vmad_fast(V3 e, float s, V3 base) {
+  return V3{fmaf(e.x, s, base.x), fmaf(e.y, s, base.y), fmaf(e.z, s, base.z)};
+}
+
+__device__ __forceinline__ V3 closest_point_triangle_fast(V3 p, V3 a, V3 b, V3 c) {
+  const V3 ab = vsub_fast(b, a);
+  const V3 ac = vsub_fast(c, a);
+  const V3 ap = vsub_fast(p, a);
+  const float d1 = vdot_fast(ab, ap);
+  const float d2 = vdot_fast(ac, ap);
+  const V3 bp = vsub_fast(p, b);
+  const float d3 = vdot_fast(ab, bp);
+  const float d4 = vdot_fast(ac, bp);
+  const V3 cq = vsub_fast(p, c);
+  const float d5 = vdot_fast(ab, cq);
+  const float d6 = vdot_fast(ac, cq);
+  const float vc = fmaf(d1, d4, -(d3 * d2));
+  const float vb = fmaf(d5, d2, -(d1 * d6));
+  const float va = fmaf(d3, d6, -(d5 * d4));
+  const float d43 = d4 - d3;
+  const float d56 = d5 - d6;
+
+  const bool rA = d1 <= 0.0f && d2 <= 0.0f;
+  const bool rB = !rA && d3 >= 0.0f && d4 <= d3;
+  const bool rAB = !rA && !rB && vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f;
+  const bool r3 = rA || rB || rAB;
+  const bool rC = !r3 && d6 >= 0.0f && d5 <= d6;
+  const bool rAC = !r3 && !rC && vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f;
+  const bool rBC = !r3 && !rC && !rAC && va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f;
+  const bool rF = !r3 && !rC && !rAC && !rBC;
+
+  float num = 0.0f, den = 1.0f;
+  if (rAB) { num = d1; den = d1 - d3; }
+  if (rAC) { num = d2; den = d2 - d6; }
+  if (rBC) { num = d43; den = d43 + d56; }
+  if (rF) { num = 1.0f; den = (va + vb) + vc; }
+  const float q = __fdividef(num, den);
+  const float s = rF ? vb * q : q;
+  const V3 base = rBC ? b : a;
+  const V3 e1 = rBC ? vsub_fast(c, b) : (rAC ? ac : ab);
+  V3 r = vmad_fast(e1, s, base);
+  if (rF) r = vmad_fast(ac, vc * q, r);
+  if (rA) r = a;
+  if (rB) r = b;
+  if (rC) r = c;
+  return r;
+}
+
+__device__ __forceinline__ float box_d2_fast(V3 p, float lox, float hix, float loy, float hiy, float loz,
+                                             float hiz) {
+  const float dx = p.x - fminf(fmaxf(p.x, lox), hix);
+  const float dy = p.y - fminf(fmaxf(p.y, loy), hiy);
+  const float dz = p.z - fminf(fmaxf(p.z, loz), hiz);
+  return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
 }
 
 __device__ __forceinline__ void cswap(float& da, int& ra, float& db, int& rb) {
@@ -123,15 +193,25 @@ struct ClosestHit {
 
 // Tests one triangle (by leaf-order slot) and keeps it if it beats the hit in
 // (d2, id) order.  Seeding a query with real candidates gives the traversal a
-// tight bound without changing its answer.
-__device__ __forceinline__ void test_slot(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
+// tight bound without changing its answer.  kFast selects the contracted-FP32
+// triangle routine (walker); callers use the test_slot / test_slot_fast wrappers.
+template <bool kFast>
+__device__ __forceinline__ void test_slot_impl(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
   const float4* t = tris + static_cast<size_t>(slot) * 3;
   const float4 a = __ldg(t + 0);
   const float4 b = __ldg(t + 1);
   const float4 c = __ldg(t + 2);
-  const V3 cp = closest_point_triangle(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z));
-  const V3 dv = vsub(cp, p);
-  const float dd = vdot(dv, dv);
+  V3 cp;
+  float dd;
+  if (kFast) {
+    cp = closest_point_triangle_fast(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z));
+    const V3 dv = vsub_fast(cp, p);
+    dd = vdot_fast(dv, dv);
+  } else {
+    cp = closest_point_triangle(p, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z));
+    const V3 dv = vsub(cp, p);
+    dd = vdot(dv, dv);
+  }
   const int id = __float_as_int(a.w);
   if (dd < hit.d2 || (dd == hit.d2 && id < hit.id)) {
     hit.d2 = dd;
@@ -139,6 +219,13 @@ __device__ __forceinline__ void test_slot(const float4* __restrict__ tris, int s
     hit.slot = slot;
     hit.cp = cp;
   }
+}
+
+__device__ __forceinline__ void test_slot(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
+  test_slot_impl<false>(tris, slot, p, hit);
+}
+__device__ __forceinline__ void test_slot_fast(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
+  test_slot_impl<true>(tris, slot, p, hit);
 }
 
 // Seed grid: (n+1)^3 lattice nodes over a padded mesh box; node value = leaf
@@ -251,7 +338,18 @@ __device__ __forceinline__ void traverse(const float4* __restrict__ nodes,
   }
 }
 
-// Per-lane state of one closest-point query in flight (stack in local memory).
+// Traversal stack in the lane's local array (kTraversalStack entries):
+// push(sp, e) stores entry sp; pop(sp) returns entry sp (the caller has
+// already decremented sp).  (A shared-memory ring holding the top 8 entries
+// measured slower: its shared-memory carve-out costs more L1 hits on node
+// fetches than it saves on pops.)
+struct LocalStack {
+  int2* a;
+  __device__ __forceinline__ void push(int sp, int2 e) { a[sp] = e; }
+  __device__ __forceinline__ int2 pop(int sp) { return a[sp]; }
+};
+
+// Per-lane state of one closest-point query in flight.
 struct TravState {
   int sp;
   int ref;       // inner node to expand next, or kEmptyChild
@@ -265,13 +363,16 @@ struct TravState {
 // pushed far-to-near, popped entries re-checked).  Returns false once the
 // query is complete.  Splitting the traversal into equal-sized steps is what
 // lets lanes with short queries move on while others are still searching.
-__device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                                          V3 p, ClosestHit& hit, TravState& t, int2* stack,
+// kFast selects the contracted-FP32 box and triangle routines (walker);
+// callers use the trav_step / trav_step_fast wrappers.
+template <bool kFast, class Stack>
+__device__ __forceinline__ bool trav_step_impl(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                          V3 p, ClosestHit& hit, TravState& t, Stack& stack,
                                           uint32_t& c_nodes, uint32_t& c_tris, bool& overflow) {
   if (t.leaf_cur >= t.leaf_end && t.ref == kEmptyChild) {
     bool found = false;
     while (t.sp > 0) {
-      const int2 e = stack[--t.sp];
+      const int2 e = stack.pop(--t.sp);
       if (__int_as_float(e.y) <= hit.d2) {
         if (e.x >= 0) {
           t.ref = e.x;
@@ -286,7 +387,7 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
     if (!found) return false;
   }
   if (t.leaf_cur < t.leaf_end) {
-    test_slot(tris, t.leaf_cur, p, hit);
+    test_slot_impl<kFast>(tris, t.leaf_cur, p, hit);
     ++t.leaf_cur;
     ++c_tris;
     return true;
@@ -300,10 +401,18 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
   const float4 hiz = __ldg(n + 5);
   const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
   ++c_nodes;
-  float d0 = box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
-  float d1 = box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
-  float d2 = box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
-  float d3 = box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
+  float d0, d1, d2, d3;
+  if (kFast) {
+    d0 = box_d2_fast(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
+    d1 = box_d2_fast(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
+    d2 = box_d2_fast(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
+    d3 = box_d2_fast(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
+  } else {
+    d0 = box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x);
+    d1 = box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y);
+    d2 = box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z);
+    d3 = box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w);
+  }
   int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
   cswap(d0, r0, d1, r1);
   cswap(d2, r2, d3, r3);
@@ -312,15 +421,15 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
   cswap(d1, r1, d2, r2);
   const float best = hit.d2;
   if (d3 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r3, __float_as_int(d3));
+    if (t.sp < kTraversalStack) stack.push(t.sp++, make_int2(r3, __float_as_int(d3)));
     else overflow = true;
   }
   if (d2 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r2, __float_as_int(d2));
+    if (t.sp < kTraversalStack) stack.push(t.sp++, make_int2(r2, __float_as_int(d2)));
     else overflow = true;
   }
   if (d1 <= best) {
-    if (t.sp < kTraversalStack) stack[t.sp++] = make_int2(r1, __float_as_int(d1));
+    if (t.sp < kTraversalStack) stack.push(t.sp++, make_int2(r1, __float_as_int(d1)));
     else overflow = true;
   }
   t.ref = kEmptyChild;
@@ -333,6 +442,17 @@ __device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, cons
     }
   }
   return true;
+}
+
+__device__ __forceinline__ bool trav_step(const float4* __restrict__ nodes, const float4* __restrict__ tris, V3 p,
+                                          ClosestHit& hit, TravState& t, LocalStack& stack, uint32_t& c_nodes,
+                                          uint32_t& c_tris, bool& overflow) {
+  return trav_step_impl<false>(nodes, tris, p, hit, t, stack, c_nodes, c_tris, overflow);
+}
+__device__ __forceinline__ bool trav_step_fast(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                               V3 p, ClosestHit& hit, TravState& t, LocalStack& stack,
+                                               uint32_t& c_nodes, uint32_t& c_tris, bool& overflow) {
+  return trav_step_impl<true>(nodes, tris, p, hit, t, stack, c_nodes, c_tris, overflow);
 }
 
 // +x ray / triangle test of the reference's slice mask

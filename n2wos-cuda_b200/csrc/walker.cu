@@ -13,10 +13,13 @@
 //    never idle a lane while work remains;
 //  * counter-based Philox keyed by (seed; walk id, step, stream), so a walk's
 //    path is independent of scheduling (serving "alone == in the mix");
-//  * the first query of every walk of a point is computed once per point; every
-//    later query is seeded with two real candidate triangles (the previous
-//    closest one and the seed-grid one at x), which bounds the traversal to the
-//    walker's neighbourhood without changing the exact (d2, id) result;
+//  * the first query of every walk of a point is computed once per point
+//    (exact arithmetic); every later query is seeded with two real candidate
+//    triangles (the previous closest one and the seed-grid one at x), which
+//    bounds the traversal to the walker's neighbourhood, and runs the
+//    contracted-FP32 box and triangle routines of geom.cuh (FMA, fast
+//    division; within a few ulps of the exact query, as the reference's own
+//    nvcc-compiled walker is);
 //  * per-point FP64 sum / sum of squares accumulated per lane over its chunk,
 //    merged across lanes with warp shuffles and flushed with FP64 atomics.
 #include <cuda_runtime.h>
@@ -177,7 +180,8 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
   hit.slot = 0;
   hit.cp = x;
   dev::TravState tv{0, kEmptyChild, 0, 0};
-  int2 stack[kTraversalStack];
+  int2 stack_mem[kTraversalStack];
+  dev::LocalStack stack{stack_mem};
 
   double acc_s = 0.0, acc_s2 = 0.0;
   uint32_t acc_n = 0, acc_forced = 0, acc_steps = 0;
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
       hit.d2 = FLT_MAX;
       hit.id = INT32_MAX;
       hit.cp = x;
-      dev::test_slot(a.tris, prev_slot, x, hit);
+      dev::test_slot_fast(a.tris, prev_slot, x, hit);
       ++c_tris;
       const dev::SeedGrid& grid = [&]() -> const dev::SeedGrid& {
         if constexpr (kBatch) return a.insts[inst].grid;
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
       if (grid.slots) {
         const int sg = dev::seed_slot(grid, x);
         if (sg != prev_slot) {
-          dev::test_slot(a.tris, sg, x, hit);
+          dev::test_slot_fast(a.tris, sg, x, hit);
           ++c_tris;
         }
       }
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
       if (busy == 0 || __popc(waiting) >= a.regen) break;
       if (querying) {
         bool ov = false;
-        if (!dev::trav_step(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
+        if (!dev::trav_step_fast(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
         if (ov) {
           w_overflow = true;
           ++c_overflow;
