@@ -184,6 +184,35 @@ __device__ __forceinline__ void cswap(float& da, int& ra, float& db, int& rb) {
   }
 }
 
+// One 4-wide node (layout.h Node4: lo_x, hi_x, lo_y, hi_y, lo_z, hi_z float4,
+// then the child refs) in four 256-bit read-only loads (ld.global.nc.v8,
+// sm_100) instead of seven 128-bit ones: a warp's divergent gathers touch
+// the same sectors with fewer L1 wavefronts.  Node arrays are cudaMalloc'd
+// (256-byte aligned) and nodes are 128 bytes, so every load is 32-byte
+// aligned.  The last load also brings the node's 16 pad bytes (same sector).
+__device__ __forceinline__ void ldg_v8f(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+__device__ __forceinline__ int4 ldg_v8_first_int4(const float4* p) {
+  int4 a;
+  int d0, d1, d2, d3;
+  asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(d0), "=r"(d1), "=r"(d2), "=r"(d3)
+      : "l"(p));
+  return a;
+}
+__device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int32_t ref, float4& lox, float4& hix,
+                                          float4& loy, float4& hiy, float4& loz, float4& hiz, int4& ch) {
+  static_assert(sizeof(Node4) == 128, "node loads assume 128-byte nodes");
+  const float4* n = nodes + static_cast<size_t>(ref) * 8;
+  ldg_v8f(n + 0, lox, hix);
+  ldg_v8f(n + 2, loy, hiy);
+  ldg_v8f(n + 4, loz, hiz);
+  ch = ldg_v8_first_int4(n + 6);
+}
+
 struct ClosestHit {
   float d2;
   int id;    // original triangle id; INT32_MAX when nothing was found below the bound
@@ -197,6 +226,8 @@ struct ClosestHit {
 // triangle routine (walker); callers use the test_slot / test_slot_fast wrappers.
 template <bool kFast>
 __device__ __forceinline__ void test_slot_impl(const float4* __restrict__ tris, int slot, V3 p, ClosestHit& hit) {
+  // three 128-bit loads: a 256-bit + 128-bit split by record parity measured
+  // slower (the selects cost more than the saved load)
   const float4* t = tris + static_cast<size_t>(slot) * 3;
   const float4 a = __ldg(t + 0);
   const float4 b = __ldg(t + 1);
@@ -392,14 +423,9 @@ __device__ __forceinline__ bool trav_step_impl(const float4* __restrict__ nodes,
     ++c_tris;
     return true;
   }
-  const float4* n = nodes + static_cast<size_t>(t.ref) * 8;
-  const float4 lox = __ldg(n + 0);
-  const float4 hix = __ldg(n + 1);
-  const float4 loy = __ldg(n + 2);
-  const float4 hiy = __ldg(n + 3);
-  const float4 loz = __ldg(n + 4);
-  const float4 hiz = __ldg(n + 5);
-  const int4 ch = __ldg(reinterpret_cast<const int4*>(n + 6));
+  float4 lox, hix, loy, hiy, loz, hiz;
+  int4 ch;
+  load_node(nodes, t.ref, lox, hix, loy, hiy, loz, hiz, ch);
   ++c_nodes;
   float d0, d1, d2, d3;
   if (kFast) {
