@@ -592,6 +592,8 @@ typedef struct n2w_server_options {
   float step_scale;        /* default 0.999 */
   int32_t block_size;      /* walker threads per block (default 256) */
   int32_t regen_threshold; /* default 8 */
+  int32_t chunk;           /* walks a lane takes per queue pop in a tick (default 1: a tick holds
+                              few walks per lane, so single walks balance the lanes best) */
 } n2w_server_options;
 
 #define N2W_STDERR_MAX 0 /* every point's standard error <= target */
@@ -645,6 +647,7 @@ typedef struct n2w_server_stats {
   int64_t pool_bytes, pool_used, peak_pool_bytes;
   int64_t nc_chunks, nc_walks; /* NC+2LMC chunks run and their coarse + residual walks */
   int64_t tick_us, nc_us;      /* worker wall time in plain ticks / NC+2LMC steps (incl. syncs) */
+  int64_t tick_gpu_us;         /* device time of the ticks' first-query + walker launches (CUDA events) */
 } n2w_server_stats;
 
 typedef struct n2w_server n2w_server;

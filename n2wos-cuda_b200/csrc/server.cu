@@ -256,6 +256,7 @@ struct n2w_server {
   double* h_conv_sum = nullptr;  // pinned
   n2w_walk_counters* h_counters = nullptr;  // pinned
   char* d_nc_scratch = nullptr;  // one chunk's coarse + residual statistics
+  cudaEvent_t ev_tick0 = nullptr, ev_tick1 = nullptr;  // brackets a tick's walker launches
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -489,7 +490,7 @@ void tick(n2w_server& s) {
     tick_points += pts;
   }
   if (slices.empty()) return;
-  const int chunk = kDefaultChunk;
+  const int chunk = s.opt.chunk > 0 ? s.opt.chunk : 1;
   int64_t cbase = 0, pbase = 0;
   for (size_t i = 0; i < slices.size(); ++i) {
     const Slice& sl = slices[i];
@@ -533,8 +534,10 @@ void tick(n2w_server& s) {
   a.counters = reinterpret_cast<n2w_walk_counters*>(s.d_hdr + 256);
   a.insts = s.d_insts;
   a.n_insts = static_cast<int>(slices.size());
+  N2W_CUDA(cudaEventRecord(s.ev_tick0, st));
   launch_first_query_batch(a, pbase, s.d_cpd, s.d_ids, st);
   launch_walker_batch(a, s.opt.block_size > 0 ? s.opt.block_size : kDefaultWalkerThreads, 0, 0, st);
+  N2W_CUDA(cudaEventRecord(s.ev_tick1, st));
   N2W_CUDA(cudaMemcpyAsync(s.h_counters, s.d_hdr + 256, sizeof(n2w_walk_counters), cudaMemcpyDeviceToHost, st));
   // Requests whose sweep ends with this tick: reduce their max stderr.
   std::vector<n2w_server::Request*> swept;
@@ -547,9 +550,12 @@ void tick(n2w_server& s) {
     launch_sweep_stderr(s, swept);
   }
   N2W_CUDA(cudaStreamSynchronize(st));
+  float tick_ms = 0.0f;
+  N2W_CUDA(cudaEventElapsedTime(&tick_ms, s.ev_tick0, s.ev_tick1));
   {
     std::lock_guard<std::mutex> lk(s.mu);
     s.stats.ticks += 1;
+    s.stats.tick_gpu_us += static_cast<int64_t>(tick_ms * 1000.0f);
     s.stats.walks += static_cast<int64_t>(s.h_counters->walks);
     s.stats.walk_steps += static_cast<int64_t>(s.h_counters->steps);
     s.stats.overflow += static_cast<int64_t>(s.h_counters->overflow);
@@ -706,6 +712,8 @@ void destroy_server(n2w_server* s) {
   cudaFreeHost(s->h_conv);
   cudaFree(s->d_conv_sum);
   cudaFree(s->d_nc_scratch);
+  if (s->ev_tick0) cudaEventDestroy(s->ev_tick0);
+  if (s->ev_tick1) cudaEventDestroy(s->ev_tick1);
   cudaFreeHost(s->h_conv_sum);
   cudaFreeHost(s->h_counters);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -732,6 +740,7 @@ int n2w_server_options_default(n2w_server_options* out) {
     out->step_scale = 0.999f;
     out->block_size = 256;
     out->regen_threshold = 8;
+    out->chunk = 1;
   });
 }
 
@@ -749,6 +758,7 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
                 "invalid walk options");
     N2W_REQUIRE(o.block_size == 0 || (o.block_size >= 32 && o.block_size <= kWalkerMaxThreads && o.block_size % 32 == 0),
                 "block_size must be 0 or a multiple of 32 in [32, 256]");
+    N2W_REQUIRE(o.chunk >= 0 && o.chunk <= 64, "chunk must be in [0, 64]");
     for (int p = 0; p < problem_count; ++p) validate_problem(problems[p]);
     s = new n2w_server();
     s->opt = o;
@@ -789,6 +799,8 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     // coarse sum, sum_sq, residual sum, sum_sq, coarse steps (8 B); coarse count, forced, residual count (4 B)
     N2W_CUDA(cudaMalloc(&s->d_nc_scratch, kNcChunk * (5 * 8 + 3 * 4)));
     N2W_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    N2W_CUDA(cudaEventCreate(&s->ev_tick0));
+    N2W_CUDA(cudaEventCreate(&s->ev_tick1));
     s->worker = std::thread(worker_loop, s);
     *out = s;
   });

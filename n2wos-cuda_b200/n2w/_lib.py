@@ -125,7 +125,8 @@ class BatchTuning(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("pool_bytes", C.c_int64), ("pool_fraction", C.c_float), ("max_inflight", C.c_int32),
                 ("tick_walks", C.c_int64), ("max_steps", C.c_int32), ("epsilon", C.c_float),
-                ("step_scale", C.c_float), ("block_size", C.c_int32), ("regen_threshold", C.c_int32)]
+                ("step_scale", C.c_float), ("block_size", C.c_int32), ("regen_threshold", C.c_int32),
+                ("chunk", C.c_int32)]
 
 
 class Request(C.Structure):
@@ -150,7 +151,7 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in
                 ("submitted", "completed", "inflight", "pending", "peak_inflight", "ticks", "walks", "walk_steps",
                  "overflow", "pool_bytes", "pool_used", "peak_pool_bytes", "nc_chunks", "nc_walks",
-                 "tick_us", "nc_us")]
+                 "tick_us", "nc_us", "tick_gpu_us")]
 
 
 N2W_REQUEST_PENDING, N2W_REQUEST_ACTIVE, N2W_REQUEST_DONE, N2W_REQUEST_CAPPED, N2W_REQUEST_FAILED = range(5)
