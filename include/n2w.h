@@ -386,6 +386,10 @@ int n2w_cache_gradients(n2w_cache* cache, const float* d_inputs, const float* d_
 int n2w_cache_train_step(n2w_cache* cache, const float* d_inputs, const float* d_targets, int64_t n,
                          float* h_loss_out, n2w_stream_t stream);
 int n2w_cache_zero_grad(n2w_cache* cache, n2w_stream_t stream);
+/* Stream-ordered device copy of the parameters (FP32 master and FP16 working
+ * copy) of src into dst, which must have the same configuration: the snapshot
+ * step of progressive estimation.  Adam state and gradients are not copied. */
+int n2w_cache_copy_params(n2w_cache* dst, const n2w_cache* src, n2w_stream_t stream);
 /* Host copies of the FP32 master parameters, the FP16 working copy and the FP32
  * gradient ([grid | mlp] order; any pointer may be NULL). */
 int n2w_cache_get_params(const n2w_cache* cache, float* h_fp32, uint16_t* h_fp16, float* h_grad);
@@ -472,6 +476,44 @@ int n2w_nc2lmc_estimate_ex(const n2w_bvh* bvh, const n2w_problem* problem, const
                            const n2w_vec3* d_points, int64_t n, const n2w_nc2lmc_options* options,
                            n2w_point_stats coarse, n2w_point_stats residual, n2w_nc2lmc_counters* d_counters,
                            n2w_stream_t stream);
+
+/* Progressive NC+2LMC with snapshot overlap (reference
+ * docs/progressive_snapshot_accounting_policy.md:30-52: evaluate snapshot k
+ * while training snapshot k+1, two cache instances, swap only at block
+ * boundaries).  For block k = 0 .. blocks-1:
+ *   1. freeze theta_infer = theta_train (n2w_cache_copy_params);
+ *   2. run one NC+2LMC block with theta_infer on eval_stream (estimate options;
+ *      block seed derived from estimate.seed and k) and add its per-point
+ *      coarse and residual sums into `coarse` / `residual`;
+ *   3. unless k is the last block, train theta_train for train_steps_per_block
+ *      steps (train options; per-block seed) on train_stream when overlap = 1,
+ *      or on eval_stream after the block when overlap = 0;
+ *   4. wait for both streams.
+ * Every block has the same coarse and residual walks per point, so the pooled
+ * estimate mean(coarse) + mean(residual) is unbiased for any sequence of
+ * snapshots, and its variance is var_c / N_c + var_r / N_r over the pooled
+ * samples.  The result does not depend on `overlap` (up to FP64 addition
+ * order).  `coarse` and `residual` are zeroed first.  h_blocks (may be NULL)
+ * receives per-block CUDA-event times.  Synchronises at every block boundary. */
+typedef struct n2w_nc_progressive_options {
+  int32_t blocks;                /* estimation blocks (one frozen snapshot each) */
+  int32_t train_steps_per_block; /* training steps theta_train takes during a block */
+  int32_t overlap;               /* 1: estimate and train on two streams; 0: serial */
+  int32_t reserved;
+  n2w_nc_train_options train;    /* `steps` is ignored */
+  n2w_nc2lmc_options estimate;   /* per-block walks */
+} n2w_nc_progressive_options;
+typedef struct n2w_nc_progressive_block {
+  float eval_ms;   /* the block's estimate on eval_stream */
+  float train_ms;  /* the block's training (0 for the last block) */
+  float wall_ms;   /* block start (snapshot copy) to both streams done */
+  float reserved;
+} n2w_nc_progressive_block;
+int n2w_nc_progressive(n2w_cache* theta_train, n2w_cache* theta_infer, const n2w_bvh* bvh,
+                       const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
+                       const n2w_nc_progressive_options* options, n2w_point_stats coarse,
+                       n2w_point_stats residual, n2w_nc_progressive_block* h_blocks,
+                       n2w_stream_t eval_stream, n2w_stream_t train_stream);
 
 /* Training labels over a fixed point set, mirroring launch_nc_update_labels
  * (include/n2wos/tcnn_nc_wos.hpp:79-86, kernel src/cuda/cubql_bvh.cu:1372-1420).

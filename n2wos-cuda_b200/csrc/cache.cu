@@ -948,6 +948,24 @@ int n2w_cache_set_params(n2w_cache* c, const float* h_fp32) {
   });
 }
 
+int n2w_cache_copy_params(n2w_cache* dst, const n2w_cache* src, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(dst && src, "null argument");
+    const n2w_cache_config& a = dst->cfg;
+    const n2w_cache_config& b = src->cfg;
+    N2W_REQUIRE(dst->n_total == src->n_total && a.n_levels == b.n_levels &&
+                    a.n_features_per_level == b.n_features_per_level && a.log2_hashmap_size == b.log2_hashmap_size &&
+                    a.base_resolution == b.base_resolution && a.per_level_scale == b.per_level_scale &&
+                    a.max_resolution == b.max_resolution && a.n_neurons == b.n_neurons &&
+                    a.n_hidden_layers == b.n_hidden_layers,
+                "n2w_cache_copy_params: caches of different configurations");
+    if (dst == src) return;
+    const size_t n = static_cast<size_t>(src->n_total);
+    N2W_CUDA(cudaMemcpyAsync(dst->d_p, src->d_p, n * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+    N2W_CUDA(cudaMemcpyAsync(dst->d_ph, src->d_ph, n * sizeof(__half), cudaMemcpyDeviceToDevice, stream));
+  });
+}
+
 int n2w_cache_zero_grad(n2w_cache* c, n2w_stream_t stream) {
   return guarded([&] {
     N2W_REQUIRE(c, "null cache");

@@ -106,4 +106,13 @@ void launch_count_samples(const uint8_t* needs, const int* forced, const int* ov
                           unsigned long long* d_counts, cudaStream_t s);
 void launch_exact(const n2w_problem& pb, const n2w_vec3* d_points, int64_t n, float* d_out, cudaStream_t s);
 
+// ---- stream-ordered scratch (util.cu) ----
+// Allocations come from a memory pool the library owns on each device, which
+// keeps up to kScratchRetainBytes cached across synchronisations, so repeated
+// calls reuse mapped memory instead of remapping it (the device's default
+// pool, left untouched, releases everything at each synchronisation).
+constexpr uint64_t kScratchRetainBytes = uint64_t{2} << 30;
+void* scratch_alloc(size_t bytes, cudaStream_t s);
+void scratch_free(void* p, cudaStream_t s);
+
 }  // namespace n2w

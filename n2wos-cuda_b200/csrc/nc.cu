@@ -48,6 +48,19 @@ __global__ void __launch_bounds__(256) sample_interior_kernel(const float4* __re
   }
 }
 
+// Adds one block's per-point statistics into running totals (fields that are
+// null in either struct are skipped).
+__global__ void accumulate_stats_kernel(n2w_point_stats part, n2w_point_stats total, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    total.d_sum[i] += part.d_sum[i];
+    total.d_sum_sq[i] += part.d_sum_sq[i];
+    total.d_count[i] += part.d_count[i];
+    if (total.d_steps && part.d_steps) total.d_steps[i] += part.d_steps[i];
+    if (total.d_forced && part.d_forced) total.d_forced[i] += part.d_forced[i];
+  }
+}
+
 // Per-point label = mean of the walks; inputs mapped to the unit cube.
 __global__ void labels_kernel(const n2w_vec3* __restrict__ pts, const double* __restrict__ sum,
                               const uint32_t* __restrict__ count, int64_t n, float3 in_min, float3 in_ext,
@@ -74,9 +87,7 @@ __global__ void map_to_unit_kernel(const n2w_vec3* __restrict__ pts, int64_t n, 
 
 template <typename T>
 T* stream_alloc(size_t count, cudaStream_t s) {
-  void* p = nullptr;
-  N2W_CUDA(cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s));
-  return static_cast<T*>(p);
+  return static_cast<T*>(scratch_alloc(std::max<size_t>(count, 1) * sizeof(T), s));
 }
 
 void sample_interior(const n2w_bvh& bvh, const float* lo, const float* hi, int64_t n, uint64_t seed,
@@ -118,7 +129,7 @@ int n2w_sample_interior_ex(const n2w_bvh* bvh, const float* box_lo, const float*
     sample_interior(*bvh, box_lo, box_hi, n, seed, d_points_out, d_c, stream);
     unsigned long long c[2] = {0, 0};
     N2W_CUDA(cudaMemcpyAsync(c, d_c, sizeof(c), cudaMemcpyDeviceToHost, stream));
-    N2W_CUDA(cudaFreeAsync(d_c, stream));
+    scratch_free(d_c, stream);
     N2W_CUDA(cudaStreamSynchronize(stream));
     const int64_t acc = static_cast<int64_t>(std::min<unsigned long long>(c[1], static_cast<unsigned long long>(n)));
     if (h_accepted_out) *h_accepted_out = acc;
@@ -191,10 +202,99 @@ int n2w_nc_train(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* proble
     for (void* p : {static_cast<void*>(pts), static_cast<void*>(inputs), static_cast<void*>(targets),
                     static_cast<void*>(sum), static_cast<void*>(sum2), static_cast<void*>(cnt),
                     static_cast<void*>(steps), static_cast<void*>(forced), static_cast<void*>(sc), ws}) {
-      cudaFreeAsync(p, stream);
+      scratch_free(p, stream);
     }
     if (status != N2W_OK) throw Error(status, err);
   });
+}
+
+int n2w_nc_progressive(n2w_cache* theta_train, n2w_cache* theta_infer, const n2w_bvh* bvh,
+                       const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
+                       const n2w_nc_progressive_options* o, n2w_point_stats coarse, n2w_point_stats residual,
+                       n2w_nc_progressive_block* h_blocks, n2w_stream_t eval_stream, n2w_stream_t train_stream) {
+  std::vector<cudaEvent_t> ev;
+  void* scratch = nullptr;
+  const int st = guarded([&] {
+    N2W_REQUIRE(theta_train && theta_infer && bvh && problem && o, "n2w_nc_progressive: null argument");
+    N2W_REQUIRE(theta_train != theta_infer, "theta_train and theta_infer must be different caches");
+    N2W_REQUIRE(o->blocks >= 1 && o->train_steps_per_block >= 0, "invalid block options");
+    N2W_REQUIRE(o->overlap == 0 || o->overlap == 1, "overlap must be 0 or 1");
+    N2W_REQUIRE(n >= 1 && d_points, "n2w_nc_progressive: need points");
+    const n2w_nc2lmc_options& eo = o->estimate;
+    N2W_REQUIRE(eo.coarse_walks >= 0 && eo.residual_walks >= 0 && (eo.coarse_walks > 0 || eo.residual_walks > 0),
+                "invalid walk counts");
+    N2W_REQUIRE(eo.coarse_walks == 0 || (coarse.d_sum && coarse.d_sum_sq && coarse.d_count), "null coarse outputs");
+    N2W_REQUIRE(eo.residual_walks == 0 || (residual.d_sum && residual.d_sum_sq && residual.d_count),
+                "null residual outputs");
+    const cudaStream_t es = eval_stream;
+    const cudaStream_t ts = o->overlap ? train_stream : eval_stream;
+    N2W_REQUIRE(!o->overlap || ts != es, "overlap needs two distinct streams");
+    auto zero = [&](const n2w_point_stats& s) {
+      if (!s.d_sum) return;
+      N2W_CUDA(cudaMemsetAsync(s.d_sum, 0, sizeof(double) * n, es));
+      N2W_CUDA(cudaMemsetAsync(s.d_sum_sq, 0, sizeof(double) * n, es));
+      N2W_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(uint32_t) * n, es));
+      if (s.d_steps) N2W_CUDA(cudaMemsetAsync(s.d_steps, 0, sizeof(uint64_t) * n, es));
+      if (s.d_forced) N2W_CUDA(cudaMemsetAsync(s.d_forced, 0, sizeof(uint32_t) * n, es));
+    };
+    zero(coarse);
+    zero(residual);
+    // one block's statistics: coarse sum, sum_sq, steps; residual sum, sum_sq, steps (8 B);
+    // coarse count, forced; residual count, forced (4 B)
+    const size_t per = static_cast<size_t>(n);
+    scratch = scratch_alloc(per * (6 * 8 + 4 * 4), es);
+    double* d = static_cast<double*>(scratch);
+    n2w_point_stats bc{d, d + per, reinterpret_cast<uint32_t*>(d + 6 * per),
+                       reinterpret_cast<uint64_t*>(d + 2 * per), reinterpret_cast<uint32_t*>(d + 6 * per) + per};
+    n2w_point_stats br{d + 3 * per, d + 4 * per, reinterpret_cast<uint32_t*>(d + 6 * per) + 2 * per,
+                       reinterpret_cast<uint64_t*>(d + 5 * per), reinterpret_cast<uint32_t*>(d + 6 * per) + 3 * per};
+    ev.resize(6);
+    for (auto& e : ev) N2W_CUDA(cudaEventCreate(&e));
+    for (int k = 0; k < o->blocks; ++k) {
+      // 1. freeze the snapshot (both streams are idle here)
+      N2W_CUDA(cudaEventRecord(ev[0], es));
+      const int rc_copy = n2w_cache_copy_params(theta_infer, theta_train, es);
+      if (rc_copy != N2W_OK) throw Error(rc_copy, n2w_last_error());
+      N2W_CUDA(cudaEventRecord(ev[1], es));
+      // 2. estimate with theta_infer
+      n2w_nc2lmc_options bo = eo;
+      bo.seed = eo.seed + 0x9E3779B97F4A7C15ull * static_cast<uint64_t>(k + 1) * 0x100000001ull;
+      const int rc_est = n2w_nc2lmc_estimate_ex(bvh, problem, theta_infer, d_points, n, &bo, bc, br, nullptr, es);
+      if (rc_est != N2W_OK) throw Error(rc_est, n2w_last_error());
+      const int g = static_cast<int>(std::min<int64_t>((n + 255) / 256, 65535));
+      if (eo.coarse_walks > 0) accumulate_stats_kernel<<<g, 256, 0, es>>>(bc, coarse, n);
+      if (eo.residual_walks > 0) accumulate_stats_kernel<<<g, 256, 0, es>>>(br, residual, n);
+      N2W_CUDA(cudaGetLastError());
+      N2W_CUDA(cudaEventRecord(ev[2], es));
+      // 3. train toward the next snapshot
+      const bool train = k + 1 < o->blocks && o->train_steps_per_block > 0;
+      N2W_CUDA(cudaEventRecord(ev[3], ts));
+      if (train) {
+        n2w_nc_train_options to = o->train;
+        to.steps = o->train_steps_per_block;
+        to.seed = o->train.seed + 0xD1B54A32D192ED03ull * static_cast<uint64_t>(k + 1);
+        const int rc_tr = n2w_nc_train(theta_train, bvh, problem, &to, nullptr, ts);
+        if (rc_tr != N2W_OK) throw Error(rc_tr, n2w_last_error());
+      }
+      N2W_CUDA(cudaEventRecord(ev[4], ts));
+      // 4. block boundary
+      N2W_CUDA(cudaStreamSynchronize(es));
+      if (ts != es) N2W_CUDA(cudaStreamSynchronize(ts));
+      if (h_blocks) {
+        float e_ms = 0.0f, t_ms = 0.0f, w0 = 0.0f, w1 = 0.0f;
+        N2W_CUDA(cudaEventElapsedTime(&e_ms, ev[1], ev[2]));
+        N2W_CUDA(cudaEventElapsedTime(&t_ms, ev[3], ev[4]));
+        N2W_CUDA(cudaEventElapsedTime(&w0, ev[0], ev[2]));
+        N2W_CUDA(cudaEventElapsedTime(&w1, ev[0], ev[4]));
+        h_blocks[k] = n2w_nc_progressive_block{e_ms, train ? t_ms : 0.0f, std::max(w0, w1), 0.0f};
+      }
+    }
+  });
+  if (scratch) cudaFreeAsync(scratch, eval_stream);  // no throw on the error path
+  for (auto& e : ev) {
+    if (e) cudaEventDestroy(e);
+  }
+  return st;
 }
 
 int n2w_nc_update_labels(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
@@ -336,7 +436,7 @@ int n2w_nc2lmc_estimate_ex(const n2w_bvh* bvh, const n2w_problem* problem, const
                     static_cast<void*>(needs), static_cast<void*>(stp), static_cast<void*>(frc),
                     static_cast<void*>(ovf), static_cast<void*>(cval), static_cast<void*>(ncv),
                     static_cast<void*>(res)}) {
-      cudaFreeAsync(p, stream);
+      scratch_free(p, stream);
     }
     if (status != N2W_OK) throw Error(status, err);
   });

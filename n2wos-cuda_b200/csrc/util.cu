@@ -11,6 +11,9 @@
 // (src/tools/eval_tcnn_nc_wos.cu:527-533), done here on the device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
+
 #include "internal.hpp"
 #include "philox.cuh"
 #include "problem.cuh"
@@ -135,6 +138,41 @@ void launch_count_samples(const uint8_t* needs, const int* forced, const int* ov
   if (n == 0) return;
   count_kernel<<<reduce_grid(n), kBlock, 0, s>>>(needs, forced, overflow, n, d_counts);
   N2W_CUDA(cudaGetLastError());
+}
+
+namespace {
+constexpr int kScratchMaxDevices = 64;
+std::mutex g_scratch_mutex;
+cudaMemPool_t g_scratch_pool[kScratchMaxDevices] = {};
+
+cudaMemPool_t scratch_pool_current_device() {
+  int dev = 0;
+  N2W_CUDA(cudaGetDevice(&dev));
+  N2W_REQUIRE(dev >= 0 && dev < kScratchMaxDevices, "device index beyond the scratch pool table");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_pool[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    N2W_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t retain = kScratchRetainBytes;
+    N2W_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &retain));
+    g_scratch_pool[dev] = pool;
+  }
+  return g_scratch_pool[dev];
+}
+}  // namespace
+
+void* scratch_alloc(size_t bytes, cudaStream_t s) {
+  void* p = nullptr;
+  N2W_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 1), scratch_pool_current_device(), s));
+  return p;
+}
+
+void scratch_free(void* p, cudaStream_t s) {
+  if (p) N2W_CUDA(cudaFreeAsync(p, s));
 }
 
 void launch_exact(const n2w_problem& pb, const n2w_vec3* d_points, int64_t n, float* d_out, cudaStream_t s) {

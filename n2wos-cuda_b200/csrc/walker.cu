@@ -693,7 +693,7 @@ void run_walker(WalkArgs& a, int64_t point_count, int out_kind, int walk_mode, c
   void* ws = d_workspace;
   bool own = false;
   if (!ws) {
-    N2W_CUDA(cudaMallocAsync(&ws, ws_bytes, stream));
+    ws = scratch_alloc(ws_bytes, stream);
     own = true;
   }
   char* base = reinterpret_cast<char*>(ws);
@@ -717,7 +717,7 @@ void run_walker(WalkArgs& a, int64_t point_count, int out_kind, int walk_mode, c
   else if (out_kind == kOutSamples) launch_walker<kOutSamples, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
   else if (walk_mode == N2W_WALK_PREFIX) launch_walker<kOutPrefix, N2W_WALK_PREFIX>(a, block, o.blocks_per_sm, stream);
   else launch_walker<kOutPrefix, N2W_WALK_RESIDUAL>(a, block, o.blocks_per_sm, stream);
-  if (own) N2W_CUDA(cudaFreeAsync(ws, stream));
+  if (own) scratch_free(ws, stream);
 }
 
 void zero_stats(const n2w_point_stats& s, int64_t n, cudaStream_t stream) {

@@ -98,6 +98,15 @@ class Nc2lmcOptions(C.Structure):
                 ("input_min", C.c_float * 3), ("input_extent", C.c_float * 3), ("point_batch", C.c_int32)]
 
 
+class NcProgressiveOptions(C.Structure):
+    _fields_ = [("blocks", C.c_int32), ("train_steps_per_block", C.c_int32), ("overlap", C.c_int32),
+                ("reserved", C.c_int32), ("train", NcTrainOptions), ("estimate", Nc2lmcOptions)]
+
+
+class NcProgressiveBlock(C.Structure):
+    _fields_ = [("eval_ms", C.c_float), ("train_ms", C.c_float), ("wall_ms", C.c_float), ("reserved", C.c_float)]
+
+
 class Nc2lmcCounters(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("coarse_cache_queries", "coarse_forced", "coarse_overflow", "residual_cache_queries",
@@ -223,6 +232,7 @@ _SIGS = {
     "n2w_cache_gradients": (I, [P, P, P, I64, P, P]),
     "n2w_cache_train_step": (I, [P, P, P, I64, C.POINTER(C.c_float), P]),
     "n2w_cache_zero_grad": (I, [P, P]),
+    "n2w_cache_copy_params": (I, [P, P, P]),
     "n2w_cache_get_params": (I, [P, P, P, P]),
     "n2w_cache_set_params": (I, [P, P]),
     "n2w_cache_save": (I, [P, C.c_char_p]),
@@ -231,6 +241,8 @@ _SIGS = {
     "n2w_sample_interior_ex": (I, [P, P, P, I64, C.c_uint64, P, C.POINTER(I64), C.POINTER(I64), P]),
     "n2w_map_to_unit": (I, [P, I64, P, P, P, P]),
     "n2w_nc_train": (I, [P, P, C.POINTER(Problem), C.POINTER(NcTrainOptions), P, P]),
+    "n2w_nc_progressive": (I, [P, P, P, C.POINTER(Problem), P, I64, C.POINTER(NcProgressiveOptions), PointStats,
+                               PointStats, P, P, P]),
     "n2w_nc2lmc_estimate": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,
                                 PointStats, P]),
     "n2w_nc2lmc_estimate_ex": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 
 from . import DeviceBuffer, PointStatsBuffers
-from ._lib import Nc2lmcOptions, NcTrainOptions, call
+from ._lib import Nc2lmcOptions, NcProgressiveBlock, NcProgressiveOptions, NcTrainOptions, call
 
 
 def input_box(mesh, pad_fraction: float = 0.05):
@@ -23,9 +23,8 @@ def input_box(mesh, pad_fraction: float = 0.05):
     return (lo - pad_fraction * ext).astype(np.float32), (ext * (1 + 2 * pad_fraction)).astype(np.float32)
 
 
-def train(cache, bvh, problem, mesh, steps=200, batch=65536, walks_per_label=32, max_steps=256, epsilon=1e-3,
-          step_scale=0.999, seed=2024, stream=None):
-    """Online training; returns the per-step batch losses."""
+def train_options(mesh, steps=200, batch=65536, walks_per_label=32, max_steps=256, epsilon=1e-3, step_scale=0.999,
+                  seed=2024):
     o = NcTrainOptions()
     o.steps, o.batch, o.walks_per_label, o.max_steps = steps, batch, walks_per_label, max_steps
     o.epsilon, o.step_scale, o.seed = epsilon, step_scale, seed
@@ -34,6 +33,13 @@ def train(cache, bvh, problem, mesh, steps=200, batch=65536, walks_per_label=32,
     for k in range(3):
         o.input_min[k], o.input_extent[k] = float(imin[k]), float(iext[k])
         o.sample_lo[k], o.sample_hi[k] = float(lo[k]), float(hi[k])
+    return o
+
+
+def train(cache, bvh, problem, mesh, steps=200, batch=65536, walks_per_label=32, max_steps=256, epsilon=1e-3,
+          step_scale=0.999, seed=2024, stream=None):
+    """Online training; returns the per-step batch losses."""
+    o = train_options(mesh, steps, batch, walks_per_label, max_steps, epsilon, step_scale, seed)
     losses = np.zeros(max(steps, 1), np.float32)
     call("n2w_nc_train", cache.handle, bvh.handle, C.byref(problem), C.byref(o), C.c_void_p(losses.ctypes.data),
          stream.handle if stream else None)
@@ -68,6 +74,39 @@ def nc2lmc(bvh, problem, cache, points, options, stream=None, d_points=None):
     c = cs.download(stream) if options.coarse_walks > 0 else None
     r = rs.download(stream) if options.residual_walks > 0 else None
     return combine(c, r, options.coarse_walks, options.residual_walks)
+
+
+def progressive(theta_train, theta_infer, bvh, problem, points, train_opts, estimate_opts, blocks=4,
+                train_steps_per_block=50, overlap=True, d_points=None):
+    """Progressive NC+2LMC (n2w_nc_progressive): block k estimates with the
+    frozen snapshot theta_k while theta_train trains toward theta_{k+1} on a
+    second stream (overlap=True) or after the block (overlap=False).  Returns
+    the pooled estimate (mean, stderr), the per-level statistics and the
+    per-block times (eval_ms, train_ms, wall_ms)."""
+    from . import Stream
+
+    if d_points is None:
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        n = len(pts)
+        d_points = DeviceBuffer.from_array(pts)
+    else:
+        n = len(points)
+    o = NcProgressiveOptions()
+    o.blocks, o.train_steps_per_block, o.overlap = blocks, train_steps_per_block, 1 if overlap else 0
+    o.train, o.estimate = train_opts, estimate_opts
+    cs, rs = PointStatsBuffers.allocate(n), PointStatsBuffers.allocate(n)
+    es, ts = Stream(), Stream()
+    out = (NcProgressiveBlock * blocks)()
+    call("n2w_nc_progressive", theta_train.handle, theta_infer.handle, bvh.handle, C.byref(problem), d_points.ptr, n,
+         C.byref(o), cs.struct(), rs.struct(), C.cast(out, C.c_void_p), es.handle, ts.handle)
+    es.sync()
+    c = cs.download(es) if estimate_opts.coarse_walks > 0 else None
+    r = rs.download(es) if estimate_opts.residual_walks > 0 else None
+    mean = (c["mean"] if c is not None else 0.0) + (r["mean"] if r is not None else 0.0)
+    var = ((c["sample_variance"] / np.maximum(c["count"], 1) if c is not None else 0.0) +
+           (r["sample_variance"] / np.maximum(r["count"], 1) if r is not None else 0.0))
+    return {"mean": mean, "estimator_variance": var, "stderr": np.sqrt(var), "coarse": c, "residual": r,
+            "blocks": [{"eval_ms": b.eval_ms, "train_ms": b.train_ms, "wall_ms": b.wall_ms} for b in out]}
 
 
 def combine(c, r, Nc, Nr):

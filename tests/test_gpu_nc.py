@@ -89,3 +89,40 @@ def test_nc_wos_only_is_biased_without_cache(gpu, scene):
     r = nc.nc2lmc(bvh, p, raw, pts, o)
     exact = problem_exact(p, pts.astype(np.float64))
     assert np.any(np.abs(r["mean"] - exact) > 10 * r["stderr"])
+
+
+def test_progressive_snapshots(gpu, scene):
+    """n2w_nc_progressive: blocks estimated with frozen snapshots while the
+    training cache advances.  Without training, overlapped and serial runs give
+    the same pooled estimate; with training, the pooled estimate is unbiased,
+    holds every block's samples, and theta_infer ends on theta_train's final
+    parameters (the last block does not train)."""
+    from n2w import nc, problem_exact
+    m, bvh = scene
+    p = gpu.problem_charges_seeded()
+    pts = np.random.default_rng(3).uniform(-0.45, 0.45, (48, 3)).astype(np.float32)
+    exact = problem_exact(p, pts.astype(np.float64))
+    cfg = gpu.cache_config(log2_hashmap_size=16, max_resolution=256.0)
+    to = nc.train_options(m, batch=8192, walks_per_label=16, epsilon=1e-3, seed=11)
+    eo = nc.nc2lmc_options(m, coarse_walks=512, residual_walks=256, depth_m=2, epsilon=1e-3, seed=5)
+    frozen = [nc.progressive(gpu.Cache(cfg), gpu.Cache(cfg), bvh, p, pts, to, eo, blocks=3,
+                             train_steps_per_block=0, overlap=ov) for ov in (True, False)]
+    np.testing.assert_allclose(frozen[0]["mean"], frozen[1]["mean"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(frozen[0]["stderr"], frozen[1]["stderr"], rtol=1e-9, atol=1e-14)
+    fresh = gpu.Cache(cfg).params()[0]
+    for overlap in (True, False):
+        theta_train, theta_infer = gpu.Cache(cfg), gpu.Cache(cfg)
+        r = nc.progressive(theta_train, theta_infer, bvh, p, pts, to, eo, blocks=3, train_steps_per_block=10,
+                           overlap=overlap)
+        assert np.all(r["coarse"]["count"] == 3 * 512) and np.all(r["residual"]["count"] == 3 * 256)
+        z = (r["mean"] - exact) / r["stderr"]
+        assert np.all(np.abs(z) < 4.5), z
+        final_train, final_infer = theta_train.params()[0], theta_infer.params()[0]
+        assert np.array_equal(final_train, final_infer)
+        assert not np.array_equal(final_train, fresh)
+        b = r["blocks"]
+        assert len(b) == 3 and b[0]["train_ms"] > 0 and b[1]["train_ms"] > 0 and b[2]["train_ms"] == 0
+        assert all(x["eval_ms"] > 0 and x["wall_ms"] >= max(x["eval_ms"], x["train_ms"]) * 0.999 for x in b)
+    with pytest.raises(gpu.N2wError):
+        same = gpu.Cache(cfg)
+        nc.progressive(same, same, bvh, p, pts, to, eo, blocks=2)
