@@ -1,6 +1,7 @@
 """GPU walkers (through the C ABI): statistical parity with the oracle's scalar
 WoS over 8 seeds, agreement with FP64 analytic solutions, per-sample vs
-per-point reduction identity, prefix/residual semantics, deadline and errors."""
+per-point reduction identity, prefix/residual semantics, deadline and errors,
+and size-independent properties of the config-1 slice at its full size."""
 import ctypes as C
 
 import numpy as np
@@ -249,3 +250,48 @@ def test_reference_analytic_modes_walk_to_exact(gpu, small_scene, name):
     assert cnt["overflow"] == 0
     exact = gpu.problem_exact(p, pts.astype(np.float64))
     assert np.all(np.abs(r["mean"] - exact) <= 4 * r["stderr"] + 2e-3), (r["mean"] - exact, r["stderr"])
+
+
+def test_config1_full_slice_properties(gpu):
+    """The config-1 workload at its full size: displaced icosphere L6 (81,920
+    triangles), the z = 0.12 slice of 512 x 512 masked to the interior, the
+    manufactured Poisson problem (sin product, omega = 3 pi), eps = 5e-4; 32
+    walks per point keep it to a fraction of a second.  Size-independent
+    properties over every point: standardized errors (mean - u) / stderr have
+    mean ~0 and variance ~1 (32-walk stderr: variance 31/29), the slice MSE
+    equals the mean estimator variance (no bias at the statistical scale), the
+    same seed reproduces every walk and step count and the means to FP64
+    rounding, and a second seed gives uncorrelated errors."""
+    m = gpu.Mesh.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345)
+    m.normalize()
+    bvh = gpu.Bvh(m, 4, "sah")
+    lo, hi = m.bounds()
+    grid, _ = gpu.slice_points(lo, hi, "xy", 0.12, 512, 512, 0.02, True)
+    pts = np.ascontiguousarray(grid[bvh.inside(grid).astype(bool)])
+    assert len(pts) > 150000
+    p = gpu.problem_sinprod(3.0 * np.pi, gpu.N2W_SOURCE_BALL)
+    exact = gpu.problem_exact(p, pts.astype(np.float64))
+    kw = dict(walks_per_point=32, epsilon=5e-4, max_steps=256)
+    a, ca = run(gpu, bvh, p, pts, seed=101, **kw)
+    b, cb = run(gpu, bvh, p, pts, seed=101, **kw)
+    c, _ = run(gpu, bvh, p, pts, seed=202, **kw)
+    assert ca["walks"] == len(pts) * 32 and ca["overflow"] == 0
+    assert np.all(a["count"] == 32)
+    assert ca["steps"] == cb["steps"] and np.array_equal(a["mean_steps"], b["mean_steps"])
+    np.testing.assert_allclose(b["mean"], a["mean"], rtol=1e-12, atol=1e-12)
+    # slice MSE over every point equals the mean estimator variance (the
+    # eps-shell bias of points next to the boundary is far below it)
+    mse = np.mean((a["mean"] - exact) ** 2)
+    ev = np.mean(a["stderr"] ** 2)
+    assert abs(mse / ev - 1.0) < 0.05, (mse, ev)
+    # standardized errors where the statistical error dominates the shell bias:
+    # points whose walks all stop at once next to the boundary have ~0 stderr
+    sel = (a["stderr"] > 0.05) & (c["stderr"] > 0.05)
+    assert sel.mean() > 0.8, sel.mean()
+    za = (a["mean"][sel] - exact[sel]) / a["stderr"][sel]
+    zc = (c["mean"][sel] - exact[sel]) / c["stderr"][sel]
+    n = int(sel.sum())
+    assert abs(za.mean()) < 5.0 / np.sqrt(n) + 0.01, za.mean()
+    assert 0.9 < za.var() < 1.3, za.var()
+    assert 0.90 < np.mean(np.abs(za) < 1.96) < 0.975, np.mean(np.abs(za) < 1.96)
+    assert abs(np.corrcoef(za, zc)[0, 1]) < 5.0 / np.sqrt(n), np.corrcoef(za, zc)[0, 1]
