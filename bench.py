@@ -486,7 +486,8 @@ def run_serve(args):
     pool_pts = [workloads.interior_ball_points(b, 65536, rng) for b in bvhs]
     problems = [n2w.problem_charges_seeded(8, 1.6, 2.0, seed=2024), n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)]
     problems[1].source_samples = args.serve_source_samples  # variance reduction of the Poisson source term
-    srv = n2w.Server(bvhs, problems, tick_walks=args.serve_tick_walks, epsilon=1e-3, chunk=args.serve_chunk)
+    srv = n2w.Server(bvhs, problems, tick_walks=args.serve_tick_walks, epsilon=1e-3, chunk=args.serve_chunk,
+                     tick_walks_max=max(args.serve_tick_walks_max, args.serve_tick_walks))
     nc_train = None
     if args.serve_nc_fraction > 0:
         from n2w import nc
@@ -608,7 +609,8 @@ def run_serve(args):
                                f"4096..{args.serve_large_max}), RMS stderr target 1e-2 (1e-3 for half of the "
                                f"<=256-point harmonic requests); {100 * args.serve_nc_fraction:.0f}% NC+2LMC "
                                "requests (icosphere, Poisson problem, pre-trained cache, m = 1, residual 1/2)",
-                   "tick_walks": args.serve_tick_walks, "chunk": args.serve_chunk or 1,
+                   "tick_walks": args.serve_tick_walks, "tick_walks_max": args.serve_tick_walks_max,
+                   "chunk": args.serve_chunk or 1,
                    "max_walks_per_point": args.serve_max_walks,
                    "seed": args.serve_seed, "time_limit_s": args.serve_time_limit},
         "complete": complete, "finished_requests": done,
@@ -657,6 +659,8 @@ def main():
                     help="Green's-function source samples per ball of the Poisson problem")
     ap.add_argument("--serve-tick-walks", type=int, default=1 << 21)
     ap.add_argument("--serve-chunk", type=int, default=0, help="walks per queue pop in a tick (0 = server default 1)")
+    ap.add_argument("--serve-tick-walks-max", type=int, default=1 << 23,
+                    help="tick budget when every request in flight has a sweep larger than --serve-tick-walks")
     ap.add_argument("--serve-seed", type=int, default=4242)
     ap.add_argument("--serve-nc-fraction", type=float, default=0.1,
                     help="fraction of requests served as NC+2LMC with a pre-trained cache")

@@ -636,6 +636,9 @@ typedef struct n2w_server_options {
   int32_t regen_threshold; /* default 8 */
   int32_t chunk;           /* walks a lane takes per queue pop in a tick (default 1: a tick holds
                               few walks per lane, so single walks balance the lanes best) */
+  int64_t tick_walks_max;  /* budget of a tick in which no request in flight could finish its
+                              sweep within tick_walks walks (default 2^23; <= tick_walks: always tick_walks):
+                              larger ticks run more efficiently but delay small requests */
 } n2w_server_options;
 
 #define N2W_STDERR_MAX 0 /* every point's standard error <= target */

@@ -464,13 +464,19 @@ void tick(n2w_server& s) {
   // The tick's walk budget goes to the requests with the least remaining
   // sweep work first (shortest remaining work first keeps small requests
   // fast); below, every request still advances by at least one point per tick.
-  const int64_t budget = s.opt.tick_walks;
   std::vector<int64_t> want(act.size()), give(act.size(), 0);
   std::vector<size_t> order(act.size());
+  bool small_in_flight = false;  // some request could finish its sweep within tick_walks
   for (size_t k = 0; k < act.size(); ++k) {
     want[k] = (act[k]->req.point_count - act[k]->cursor) * static_cast<int64_t>(act[k]->sweep_walks);
     order[k] = k;
+    small_in_flight = small_in_flight || want[k] <= s.opt.tick_walks;
   }
+  // Larger ticks when only large sweeps are in flight: a tick waits for its
+  // slowest walk, so more walks per tick fill the GPU better, and no small
+  // request is there to be delayed by the longer tick.
+  const int64_t budget = (!small_in_flight && s.opt.tick_walks_max > s.opt.tick_walks) ? s.opt.tick_walks_max
+                                                                                          : s.opt.tick_walks;
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return want[a] < want[b]; });
   int64_t left = budget;
   for (size_t k : order) {
@@ -741,6 +747,7 @@ int n2w_server_options_default(n2w_server_options* out) {
     out->block_size = 256;
     out->regen_threshold = 8;
     out->chunk = 1;
+    out->tick_walks_max = int64_t{1} << 23;
   });
 }
 
@@ -759,6 +766,7 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     N2W_REQUIRE(o.block_size == 0 || (o.block_size >= 32 && o.block_size <= kWalkerMaxThreads && o.block_size % 32 == 0),
                 "block_size must be 0 or a multiple of 32 in [32, 256]");
     N2W_REQUIRE(o.chunk >= 0 && o.chunk <= 64, "chunk must be in [0, 64]");
+    N2W_REQUIRE(o.tick_walks_max >= 0, "tick_walks_max must be >= 0 (values <= tick_walks disable larger ticks)");
     for (int p = 0; p < problem_count; ++p) validate_problem(problems[p]);
     s = new n2w_server();
     s->opt = o;
@@ -784,8 +792,8 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     s->pool = std::make_unique<PoolAllocator>(pool);
     s->opt.pool_bytes = static_cast<int64_t>(pool);
     // A tick holds at most one instance per in-flight request and at most
-    // tick_walks / 32 + max_inflight points (sweeps have >= 32 walks per point).
-    s->tick_point_cap = o.tick_walks / 32 + o.max_inflight;
+    // (its budget) / 32 + max_inflight points (sweeps have >= 32 walks per point).
+    s->tick_point_cap = std::max(o.tick_walks, o.tick_walks_max) / 32 + o.max_inflight;
     N2W_CUDA(cudaMalloc(&s->d_insts, sizeof(BatchInst) * o.max_inflight));
     N2W_CUDA(cudaMallocHost(&s->h_insts, sizeof(BatchInst) * o.max_inflight));
     N2W_CUDA(cudaMalloc(&s->d_cpd, sizeof(float4) * s->tick_point_cap));

@@ -135,7 +135,7 @@ class ServerOptions(C.Structure):
     _fields_ = [("pool_bytes", C.c_int64), ("pool_fraction", C.c_float), ("max_inflight", C.c_int32),
                 ("tick_walks", C.c_int64), ("max_steps", C.c_int32), ("epsilon", C.c_float),
                 ("step_scale", C.c_float), ("block_size", C.c_int32), ("regen_threshold", C.c_int32),
-                ("chunk", C.c_int32)]
+                ("chunk", C.c_int32), ("tick_walks_max", C.c_int64)]
 
 
 class Request(C.Structure):

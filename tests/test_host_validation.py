@@ -18,7 +18,7 @@ def test_server_option_defaults(n2w):
     call("n2w_server_options_default", C.byref(o))
     assert (o.pool_bytes, o.max_inflight, o.tick_walks, o.max_steps) == (0, 256, 1 << 21, 256)
     assert abs(o.pool_fraction - 0.25) < 1e-7 and abs(o.epsilon - 1e-3) < 1e-9
-    assert (o.block_size, o.regen_threshold, o.chunk) == (256, 8, 1)
+    assert (o.block_size, o.regen_threshold, o.chunk, o.tick_walks_max) == (256, 8, 1, 1 << 23)
 
 
 def test_server_create_rejects_bad_options(n2w):
@@ -29,7 +29,7 @@ def test_server_create_rejects_bad_options(n2w):
     out = C.c_void_p()
     for field, value, needle in (("chunk", 65, "chunk"), ("max_inflight", 0, "max_inflight"),
                                  ("tick_walks", 16, "tick_walks"), ("block_size", 48, "block_size"),
-                                 ("epsilon", 0.0, "walk options")):
+                                 ("epsilon", 0.0, "walk options"), ("tick_walks_max", -1, "tick_walks_max")):
         o = ServerOptions()
         call("n2w_server_options_default", C.byref(o))
         setattr(o, field, value)
