@@ -31,8 +31,12 @@ namespace {
 // Persistent state machine, one lane per query.  Every iteration each busy
 // lane advances its query by ONE unit of traversal work (one 4-wide node
 // expansion or one triangle test, dev::trav_step), and a lane whose query is
-// complete writes it and takes the next query of a grid-stride sequence in
-// the same iteration.  Lanes therefore never wait for another lane's whole
+// complete writes it and takes the next query in the same iteration.  Each
+// block owns the contiguous range [b n / B, (b + 1) n / B) of the queries and
+// its lanes take them from a shared-memory counter as they finish, so a lane
+// that drew slow queries does not hold up queries that idle lanes of its
+// block could run (with a fixed grid-stride sequence, launches of ~1-2
+// queries per lane last as long as their unluckiest lane's pair).  Lanes therefore never wait for another lane's whole
 // traversal (one-query-per-thread loops leave ~3.6 of 32 lanes active on
 // incoherent queries); short work units keep the warp's two code paths
 // (node / triangle) busy.  The visit order, pruning and pushes are those of
@@ -46,9 +50,14 @@ __global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
     const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
     float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
     int* __restrict__ out_overflow, int* __restrict__ out_nodes, int* __restrict__ out_tris) {
-  const int stride = gridDim.x * blockDim.x;
-  int q = blockIdx.x * blockDim.x + threadIdx.x - stride;  // advanced before first use
-  bool busy = false;
+  // next unclaimed query of this block's range (unsigned: after the range
+  // runs out each lane claims once more, up to b_end + blockDim.x <= 2^31 + 1023)
+  __shared__ unsigned s_next;
+  const unsigned b_end = static_cast<unsigned>((static_cast<int64_t>(blockIdx.x) + 1) * n / gridDim.x);
+  if (threadIdx.x == 0) s_next = static_cast<unsigned>(static_cast<int64_t>(blockIdx.x) * n / gridDim.x);
+  __syncthreads();
+  int q = 0;
+  bool busy = false, drained = false;
   dev::V3 p = dev::v3(0.0f, 0.0f, 0.0f);
   dev::ClosestHit hit;
   hit.d2 = FLT_MAX;
@@ -61,9 +70,13 @@ __global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
   uint32_t c_nodes = 0, c_tris = 0;
   bool overflow = false;
   for (;;) {
-    while (!busy) {
-      q += stride;
-      if (q >= n) break;
+    while (!busy && !drained) {
+      const unsigned claim = atomicAdd(&s_next, 1u);
+      if (claim >= b_end) {
+        drained = true;  // stop claiming
+        break;
+      }
+      q = static_cast<int>(claim);
       const n2w_vec3 pt = points[q];
       if (kMasked && active[q] == 0) {
         out_d2[q] = 0.0f;
@@ -167,8 +180,8 @@ void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const ui
                           int n, float* d_d2, n2w_vec3* d_cp, int* d_id, int* d_overflow,
                           int* d_nodes, int* d_tris, int block_size, cudaStream_t stream) {
   // block_size (the reference's launch knob, validated to [1, 1024]) is a hint:
-  // the kernel runs 256-thread blocks over a grid-stride loop sized to the
-  // resident capacity of the GPU.
+  // the kernel runs 256-thread blocks, each over its own range of the queries,
+  // with the grid sized to the resident capacity of the GPU.
   (void)block_size;
   const float4* nodes = reinterpret_cast<const float4*>(bvh.d_nodes);
   const float4* tris = reinterpret_cast<const float4*>(bvh.d_tris);
