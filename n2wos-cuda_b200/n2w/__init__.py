@@ -388,6 +388,21 @@ def walk_options(walks_per_point=256, max_steps=256, depth_m=8, epsilon=1e-3, st
     return o
 
 
+def label_options(walks_per_point=32, max_steps=256, epsilon=1e-3, step_scale=0.999, seed=12345, refresh_index=0,
+                  label_source=1, input_min=(0.0, 0.0, 0.0), input_extent=(1.0, 1.0, 1.0), block_size=0):
+    """n2w_nc_label_options: one refresh of n2w_nc_update_labels (label_source
+    1 = WoS walks, 0 = the exact solution)."""
+    from ._lib import NcLabelOptions
+
+    o = NcLabelOptions()
+    o.walks_per_point, o.max_steps, o.epsilon, o.step_scale = walks_per_point, max_steps, epsilon, step_scale
+    o.seed, o.refresh_index, o.label_source, o.block_size = seed, refresh_index, label_source, block_size
+    for k in range(3):
+        o.input_min[k] = float(input_min[k])
+        o.input_extent[k] = float(input_extent[k])
+    return o
+
+
 @dataclass
 class PointStatsBuffers:
     n: int

@@ -125,6 +125,10 @@ class RefMesh:
     def degenerate_count(self):
         return int(ref().ref_count_degenerate(self.h))
 
+    def host_bvh(self, leaf_size=8):
+        """The reference's own host BVH (build_host_bvh, median split)."""
+        return RefHostBvh(self, leaf_size)
+
     def host_bvh_stats(self, leaf_size=8):
         n, d = C.c_int64(), C.c_int32()
         if ref().ref_host_bvh_stats(self.h, leaf_size, C.byref(n), C.byref(d)) != 0:
@@ -135,6 +139,38 @@ class RefMesh:
         if getattr(self, "h", None) and _ref is not None:
             _ref.ref_mesh_free(self.h)
             self.h = None
+
+
+class RefHostBvh:
+    """Arrays of the reference's host BVH (src/cuda/bvh_build_host.cpp): 36-byte
+    triangles, 40-byte nodes (box, left, right, first, count), leaf index list."""
+
+    TRI = np.dtype([("v", np.float32, (3, 3))])
+    NODE = np.dtype([("lo", np.float32, 3), ("hi", np.float32, 3), ("left", np.int32), ("right", np.int32),
+                     ("first", np.int32), ("count", np.int32)])
+
+    def __init__(self, mesh: "RefMesh", leaf_size: int = 8):
+        R = ref()
+        R.ref_host_bvh_build.restype = C.c_void_p
+        R.ref_host_bvh_build.argtypes = [C.c_void_p, C.c_int]
+        R.ref_host_bvh_counts.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 3 + [C.POINTER(C.c_int32)]
+        R.ref_host_bvh_copy.argtypes = [C.c_void_p] * 4
+        R.ref_host_bvh_free.argtypes = [C.c_void_p]
+        h = R.ref_host_bvh_build(mesh.h, leaf_size)
+        if not h:
+            raise RuntimeError(R.ref_last_error().decode())
+        nt, nn, ni, dep = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        R.ref_host_bvh_counts(h, C.byref(nt), C.byref(nn), C.byref(ni), C.byref(dep))
+        self.tris = np.empty(nt.value, self.TRI)
+        self.nodes = np.empty(nn.value, self.NODE)
+        self.idx = np.empty(ni.value, np.int32)
+        R.ref_host_bvh_copy(h, _p(self.tris), _p(self.nodes), _p(self.idx))
+        R.ref_host_bvh_free(h)
+        self.leaf_size = leaf_size
+        self.depth = dep.value
+
+    def args(self):
+        return _p(self.nodes), _p(self.tris), _p(self.idx)
 
 
 def ref_gpu_available() -> bool:
@@ -168,6 +204,20 @@ def _setup():
     L.oracle_wos.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                              C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_int]
+    L.oracle_wos_ref_bvh.argtypes = [C.c_void_p] * 5 + [C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float,
+                                                        C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                        C.c_int]
+    L.oracle_ref_bvh_query.argtypes = [C.c_void_p] * 4 + [C.c_int64] + [C.c_void_p] * 5 + [C.c_int]
+    L.oracle_inside_ref_bvh.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_void_p, C.c_int]
+    L.oracle_walk_samples.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                                        C.c_float, C.c_uint32, C.c_uint32] + [C.c_void_p] * 8 + [C.c_int]
+    L.oracle_nc_combine.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_void_p, C.c_void_p]
+    L.oracle_nc_update_labels.argtypes = [C.c_void_p] * 4 + [C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float,
+                                                            C.c_uint32, C.c_uint32, C.c_int] + [C.c_void_p] * 5 + [C.c_int]
+    L.oracle_icosphere_displaced.argtypes = [C.c_int, C.c_float, C.c_float, C.c_int, C.c_float, C.c_uint64,
+                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p, C.c_void_p]
+    L.oracle_slice_points.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int,
+                                      C.c_void_p, C.c_void_p]
     return L
 
 
@@ -256,3 +306,133 @@ def wos(nodes, tris, problem_bytes, points, walks_per_point, max_steps, eps, ste
     var = np.maximum((s2 - W * mean * mean) / max(W - 1, 1), 0.0)
     return {"mean": mean, "sample_variance": var, "stderr": np.sqrt(var / W), "mean_steps": st / W,
             "sum": s, "sum_sq": s2, "steps": st}
+
+
+# ---- the reference path on the CPU: its host BVH, the walk, the slice mask -----
+
+def _moments(s, s2, st, W):
+    W = float(W)
+    mean = s / W
+    var = np.maximum((s2 - W * mean * mean) / max(W - 1, 1), 0.0)
+    return {"mean": mean, "sample_variance": var, "stderr": np.sqrt(var / W), "mean_steps": st / W,
+            "sum": s, "sum_sq": s2, "steps": st}
+
+
+def wos_ref_bvh(bvh: RefHostBvh, problem_bytes, points, walks_per_point, max_steps, eps, step_scale, k0, k1,
+                threads=8):
+    """Scalar CPU WoS over the reference's own host BVH (reference
+    nc_wos_from_point semantics, closest points by the restated
+    closest_point_bvh_kernel traversal); per-point FP64 sums."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    n = len(pts)
+    s, s2, st = (np.empty(n, np.float64) for _ in range(3))
+    pb = np.frombuffer(problem_bytes, dtype=np.uint8).copy()
+    L.oracle_wos_ref_bvh(*bvh.args(), _p(pb), _p(pts), n, walks_per_point, max_steps, eps, step_scale, k0, k1,
+                         _p(s), _p(s2), _p(st), threads)
+    return _moments(s, s2, st, walks_per_point)
+
+
+def ref_bvh_query(bvh: RefHostBvh, points, threads=8):
+    """Closest point over the reference's host BVH (restated bvh_query.cu:75-160)."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    n = len(pts)
+    d2 = np.empty(n, np.float32)
+    cp = np.empty((n, 3), np.float32)
+    ids, nv, nt = (np.empty(n, np.int32) for _ in range(3))
+    L.oracle_ref_bvh_query(*bvh.args(), _p(pts), n, _p(d2), _p(cp), _p(ids), _p(nv), _p(nt), threads)
+    return {"distance2": d2, "closest": cp, "triangle_id": ids, "node_visits": nv, "tri_tests": nt}
+
+
+def inside_ref_bvh(bvh: RefHostBvh, points, threads=8):
+    """Reference +x ray-parity mask (cubql_bvh.cu:446-455), culled by the
+    reference BVH's boxes (same hit count as the brute force)."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    out = np.empty(len(pts), np.uint8)
+    L.oracle_inside_ref_bvh(*bvh.args(), _p(pts), len(pts), _p(out), threads)
+    return out
+
+
+MODE_PURE, MODE_PREFIX, MODE_RESIDUAL = 0, 1, 2
+
+
+def walk_samples(nodes, tris, problem_bytes, points, walks_per_point, mode, depth_m, max_steps, eps, step_scale,
+                 k0, k1, input_min=None, input_extent=None, threads=8):
+    """Per-sample walks (sample i*W + j) restating nc_pure_wos_samples_kernel
+    (mode 0), nc_hybrid_prefix_kernel (1) and nc_2lmc_prefix_continue_kernel (2)
+    of cubql_bvh.cu:1422-1606."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    S = len(pts) * walks_per_point
+    value, cont = np.empty(S, np.float32), np.empty(S, np.float32)
+    inputs = np.empty((S, 3), np.float32)
+    needs = np.empty(S, np.uint8)
+    steps, forced = np.empty(S, np.int32), np.empty(S, np.int32)
+    lo = np.ascontiguousarray(input_min if input_min is not None else np.zeros(3), np.float32)
+    ext = np.ascontiguousarray(input_extent if input_extent is not None else np.ones(3), np.float32)
+    pb = np.frombuffer(problem_bytes, dtype=np.uint8).copy()
+    L.oracle_walk_samples(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(tris)), _p(pb), _p(pts), len(pts),
+                          walks_per_point, mode, depth_m, max_steps, eps, step_scale, k0, k1, _p(lo), _p(ext),
+                          _p(value), _p(cont), _p(inputs), _p(needs), _p(steps), _p(forced), threads)
+    return {"value": value, "continuation": cont, "inputs": inputs, "needs_cache": needs, "steps": steps,
+            "forced": forced}
+
+
+def nc_combine(cache_out, boundary, cont, needs):
+    """nc_combine_cache_and_residual_kernel (cubql_bvh.cu:1608-1627)."""
+    L = _setup()
+    c = np.ascontiguousarray(cache_out, np.float32)
+    b = np.ascontiguousarray(boundary, np.float32)
+    w = np.ascontiguousarray(cont, np.float32)
+    nd = np.ascontiguousarray(needs, np.uint8)
+    nc, res = np.empty(len(c), np.float32), np.empty(len(c), np.float32)
+    L.oracle_nc_combine(_p(c), _p(b), _p(w), _p(nd), len(c), _p(nc), _p(res))
+    return nc, res
+
+
+def nc_update_labels(nodes, tris, problem_bytes, points, walks_per_point, max_steps, eps, step_scale, k0, k1,
+                     label_source, input_min, input_extent, targets, counts, threads=8):
+    """One refresh of nc_update_labels_kernel (cubql_bvh.cu:1372-1420); updates
+    `targets` (float32) and `counts` (int32) in place, returns the inputs."""
+    L = _setup()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    assert targets.dtype == np.float32 and counts.dtype == np.int32 and targets.flags.c_contiguous
+    inputs = np.empty((len(pts), 3), np.float32)
+    pb = np.frombuffer(problem_bytes, dtype=np.uint8).copy()
+    lo = np.ascontiguousarray(input_min, np.float32)
+    ext = np.ascontiguousarray(input_extent, np.float32)
+    L.oracle_nc_update_labels(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(tris)), _p(pb), _p(pts),
+                              len(pts), walks_per_point, max_steps, eps, step_scale, k0, k1, label_source, _p(lo),
+                              _p(ext), _p(inputs), _p(targets), _p(counts), threads)
+    return inputs
+
+
+def icosphere_displaced(level=6, amplitude=0.12, base_frequency=3.0, octaves=4, persistence=0.5, seed=12345):
+    """The displaced icosphere of the Poisson slice workload (unnormalised)."""
+    L = _setup()
+    nv, nt = C.c_int64(), C.c_int64()
+    L.oracle_icosphere_displaced(level, amplitude, base_frequency, octaves, persistence, seed, C.byref(nv),
+                                 C.byref(nt), None, None)
+    v = np.empty((nv.value, 3), np.float32)
+    t = np.empty((nt.value, 3), np.uint32)
+    L.oracle_icosphere_displaced(level, amplitude, base_frequency, octaves, persistence, seed, C.byref(nv),
+                                 C.byref(nt), _p(v), _p(t))
+    return v, t
+
+
+SLICE_RULE_RENDER, SLICE_RULE_EVAL = 0, 1
+
+
+def slice_points(bounds6, view="xy", plane=0.0, width=512, height=512, padding=0.02, preserve_aspect=True,
+                 rule=SLICE_RULE_RENDER):
+    """Slice pixel grid of the reference's render / evaluation tools."""
+    L = _setup()
+    b = np.ascontiguousarray(bounds6, np.float32)
+    pts = np.empty((height * width, 3), np.float32)
+    frame = np.empty(4, np.float32)
+    if L.oracle_slice_points(_p(b), {"xy": 0, "xz": 1, "yz": 2}[view], plane, width, height, padding,
+                             int(preserve_aspect), rule, _p(pts), _p(frame)) != 0:
+        raise ValueError("bad slice view")
+    return pts, frame

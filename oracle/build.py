@@ -10,6 +10,13 @@
 * ``oracle/_ref/libn2wos_ref_gpu.so``: the reference's in-tree GPU kernel
   (src/cuda/bvh_query.cu + bvh_build_host.cpp) compiled unmodified for sm_100a,
   plus ref_gpu_shim.cu.
+* ``oracle/_ref/meshes/bunny_zipper_wataertight.ply``: a copy of the reference's
+  bundled bunny mesh (data the GPU checks load where the checkout is absent).
+
+The reference checkout is located by ``reference_root()``: the environment
+variable N2W_REFERENCE_ROOT when set, else the checkout's default location.
+Everything under oracle/_ref is a build output: never committed, but it travels
+with the repository snapshot to GPU machines.
 
 The reference's cuBQL / tiny-cuda-nn targets are not buildable (those
 third-party sources are not vendored), so they are not attempted.
@@ -17,13 +24,20 @@ third-party sources are not vendored), so they are not attempted.
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
-REFERENCE = Path(os.environ.get("N2W_REFERENCE_ROOT", "/root/reference"))
+DEFAULT_REFERENCE_ROOT = "/root/reference"
+REF_BUNNY = REF_OUT / "meshes" / "bunny_zipper_wataertight.ply"
+
+
+def reference_root() -> Path:
+    """The reference checkout: $N2W_REFERENCE_ROOT, else the default location."""
+    return Path(os.environ.get("N2W_REFERENCE_ROOT", DEFAULT_REFERENCE_ROOT))
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 REF_CPU_SOURCES = ["src/mesh/normalize.cpp", "src/mesh/ply_loader.cpp", "src/mesh/obj_loader.cpp",
@@ -55,9 +69,14 @@ def build_oracle() -> Path:
 
 def build_ref() -> list[Path]:
     """Builds oracle/_ref from the reference sources when they are present."""
+    REFERENCE = reference_root()
     if not (REFERENCE / "src").is_dir():
         return []
     REF_OUT.mkdir(exist_ok=True)
+    bunny = REFERENCE / "meshes" / REF_BUNNY.name
+    if bunny.exists() and _stale(REF_BUNNY, [bunny]):
+        REF_BUNNY.parent.mkdir(exist_ok=True)
+        shutil.copyfile(bunny, REF_BUNNY)
     inc = [f"-I{REFERENCE / 'include'}", f"-I{REFERENCE / 'src' / 'cuda'}", f"-I{CUDA_HOME / 'include'}"]
     built = []
     cpu = REF_OUT / "libn2wos_ref.so"

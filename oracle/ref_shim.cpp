@@ -124,6 +124,36 @@ int ref_host_bvh_stats(void* h, int leaf_size, int64_t* nodes, int32_t* depth) {
   }
 }
 
+// The reference host BVH itself (bvh_build_host.cpp:129-158): triangles in
+// mesh order (36 B each), nodes in DFS order (40 B each), the leaf triangle
+// index list.  Walked by the oracle's restatement of closest_point_bvh_kernel.
+void* ref_host_bvh_build(void* h, int leaf_size) {
+  try {
+    return new n2wos::HostBvhData(n2wos::build_host_bvh(*as_mesh(h), leaf_size));
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+void ref_host_bvh_counts(void* b, int64_t* tris, int64_t* nodes, int64_t* idx, int32_t* depth) {
+  const auto* d = static_cast<const n2wos::HostBvhData*>(b);
+  *tris = static_cast<int64_t>(d->triangles.size());
+  *nodes = static_cast<int64_t>(d->nodes.size());
+  *idx = static_cast<int64_t>(d->triangle_indices.size());
+  *depth = d->max_depth;
+}
+
+void ref_host_bvh_copy(void* b, void* tris, void* nodes, int32_t* idx) {
+  const auto* d = static_cast<const n2wos::HostBvhData*>(b);
+  static_assert(sizeof(n2wos::DeviceTriangle) == 36 && sizeof(n2wos::DeviceBvhNode) == 40, "reference layout");
+  std::memcpy(tris, d->triangles.data(), d->triangles.size() * sizeof(n2wos::DeviceTriangle));
+  std::memcpy(nodes, d->nodes.data(), d->nodes.size() * sizeof(n2wos::DeviceBvhNode));
+  for (size_t i = 0; i < d->triangle_indices.size(); ++i) idx[i] = d->triangle_indices[i];
+}
+
+void ref_host_bvh_free(void* b) { delete static_cast<n2wos::HostBvhData*>(b); }
+
 // Boundary data u and source f of the reference's header-only analytic modes
 // (harmonic mixtures 13-16, manufactured Poisson 30, 31, 32), evaluated by the
 // reference's own inline functions.  Returns 0, or -1 for another mode.

@@ -19,7 +19,17 @@ for p in (str(ROOT), str(PKG)):
         sys.path.insert(0, p)
 
 GOLDEN = ROOT / "tests" / "golden"
-REFERENCE_BUNNY = Path("/root/reference/meshes/bunny_zipper_wataertight.ply")
+
+
+def _reference_bunny() -> Path:
+    """The reference's bunny PLY: the copy oracle/build.py stages in oracle/_ref
+    (it travels to GPU machines), else the reference checkout's own file."""
+    from oracle import build as ob
+
+    return ob.REF_BUNNY if ob.REF_BUNNY.exists() else ob.reference_root() / "meshes" / ob.REF_BUNNY.name
+
+
+REFERENCE_BUNNY = _reference_bunny()
 
 
 def pytest_configure(config):

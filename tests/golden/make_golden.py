@@ -31,8 +31,9 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
 import oracle  # noqa: E402
+from oracle import build as ob  # noqa: E402
 
-BUNNY = Path("/root/reference/meshes/bunny_zipper_wataertight.ply")
+BUNNY = ob.reference_root() / "meshes" / "bunny_zipper_wataertight.ply"
 
 
 def sha(a: np.ndarray) -> str:
