@@ -135,44 +135,210 @@ def build_scene(n2w, lib, call):
     return mesh, bvh, pts, problem, exact, frame
 
 
-def cpu_port_sample(n2w, bvh_or_layout, problem, pts, walks, seconds_target=12.0, threads=None):
-    """Times the oracle's scalar WoS port on a bounded prefix of the points."""
+REF_SAMPLE_STRIDE = 256  # the CPU legs walk every 256th interior slice point
+
+
+def loaded_libraries() -> list[str]:
+    """Shared objects of this repository mapped into the process (/proc/self/maps)."""
+    found = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            path = line.split()[-1] if line.split() else ""
+            if path.endswith(".so") and path.startswith(str(ROOT)):
+                found.add(str(Path(path).relative_to(ROOT)))
+    except OSError:
+        pass
+    return sorted(found)
+
+
+def reference_cpu_scene():
+    """The headline workload rebuilt without the product library: the oracle's
+    displaced icosphere, normalised by the reference's own normalize_to_unit_radius
+    and indexed by the reference's own median-split host BVH (leaf 8), both from
+    its sources compiled into oracle/_ref; the slice grid and the reference's
+    ray-parity mask from the oracle; the sin-product problem record."""
     import oracle
 
-    nodes, tris = bvh_or_layout
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref (the reference's CPU sources) is not built")
+    v, t = oracle.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345)
+    rm = oracle.RefMesh.from_arrays(v, t)
+    rm.normalize()
+    v, t = rm.arrays()
+    bvh = rm.host_bvh(8)
+    b6 = np.concatenate([v.min(0), v.max(0)]).astype(np.float32)
+    grid, _ = oracle.slice_points(b6, "xy", 0.12, 512, 512, 0.02, True, oracle.SLICE_RULE_RENDER)
+    pts = np.ascontiguousarray(grid[oracle.inside_ref_bvh(bvh, grid).astype(bool)])
+    problem = oracle.problem_record(101, 0, np.float32(3.0 * np.pi), 0)
+    return bvh, pts, problem
+
+
+def reference_cpu_sample(scene, walks, seed=12345, threads=None):
+    """The reference path's CPU form on a fixed sample of the workload: every
+    REF_SAMPLE_STRIDE-th interior slice point x `walks` walks, the oracle's port
+    of nc_wos_from_point (src/cuda/cubql_bvh.cu:1323-1357) whose closest points
+    come from its port of closest_point_bvh_kernel (src/cuda/bvh_query.cu:75-160)
+    over the reference's host BVH, on all host threads."""
+    import oracle
+
+    bvh, pts, problem = scene
+    sel = np.ascontiguousarray(pts[::REF_SAMPLE_STRIDE])
     threads = threads or os.cpu_count() or 1
-    # calibration on an evenly spread set of points (walk cost depends on the
-    # distance to the boundary), then a sample sized for ~seconds_target
-    cal = pts[np.linspace(0, len(pts) - 1, max(64, 4 * threads)).astype(np.int64)]
     t0 = time.perf_counter()
-    oracle.wos(nodes, tris, bytes(problem), cal, walks, 256, 5e-4, 0.999, 12345, 0, threads)
-    dt = time.perf_counter() - t0
-    per_point = max(dt, 1e-6) / len(cal)  # wall seconds per point with all threads busy
-    n = int(np.clip(seconds_target / per_point, threads, len(pts)))
-    sel = pts[np.linspace(0, len(pts) - 1, n).astype(np.int64)]
-    t0 = time.perf_counter()
-    r = oracle.wos(nodes, tris, bytes(problem), sel, walks, 256, 5e-4, 0.999, 12345, 0, threads)
+    r = oracle.wos_ref_bvh(bvh, problem, sel, walks, 256, 5e-4, 0.999, seed & 0xFFFFFFFF, seed >> 32, threads)
     dt = time.perf_counter() - t0
     steps = float(r["steps"].sum())
     return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} of {len(pts)} slice points x {walks} walks ({steps:.3g} walk-steps) in {dt:.1f} s"}
+            "sample": (f"every {REF_SAMPLE_STRIDE}th of the {len(pts)} interior slice points ({len(sel)} points) x "
+                       f"{walks} walks = {steps:.4g} walk-steps in {dt:.2f} s; reference median-split host BVH "
+                       "(leaf 8, bvh_build_host.cpp built from its sources) walked by the oracle's ports of "
+                       "closest_point_bvh_kernel and nc_wos_from_point")}
 
 
-def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub=16384, train_steps=200):
+def cache_level_peaks(call):
+    """L1 and L2 read bandwidth measured live by the library's own probe kernels
+    (n2w_probe_read_bandwidth): the denominators for the traversal's bytes,
+    which are L1 / L2 hits, beside the HBM copy peak."""
+    out = {}
+    for level, key, nbytes, iters in ((1, "l1_gbs", 0, 4096), (2, "l2_gbs", 32 << 20, 64)):
+        g = C.c_double()
+        try:
+            call("n2w_probe_read_bandwidth", level, nbytes, iters, C.byref(g))
+            out[key] = g.value
+        except Exception as e:  # a probe failure must not break the bench line
+            out[key] = None
+            out[key + "_error"] = str(e)
+    return out
+
+
+def fractions(achieved_gbs, hbm_peak, cache_peaks):
+    fr = {"hbm": achieved_gbs / hbm_peak}
+    for key, lvl in (("l2_gbs", "l2"), ("l1_gbs", "l1")):
+        if cache_peaks.get(key):
+            fr[lvl] = achieved_gbs / cache_peaks[key]
+    return fr
+
+
+def closest_point_segment(n2w, call, stream, timer, flush, cache_peaks, repeat=20, validate=2048,
+                          reference_kernel=True, n=262144):
+    """Config-0 closest-point queries: 262,144 points uniform in [-1.2, 1.2]^3
+    (PCG64 seed 12345) on the bumpy sphere r = 1 + 0.08 sin(6 theta) cos(8 phi),
+    128 x 256 (65,024 triangles), normalised; 4-wide SAH BVH, leaves of <= 4.
+    Each timed launch of n2w_bvh_query_device follows a 256 MiB L2 flush and is
+    timed with CUDA events on its stream.  Algorithmic bytes per query:
+    12 in + 28 out + node visits x 128 + triangle tests x 48 (counts from the
+    counting variant of the same traversal).  Beside it, as a baseline, the
+    reference's own closest_point_bvh_kernel (src/cuda/bvh_query.cu:75-160,
+    median-split BVH, leaf 8, block 128), compiled from its sources for sm_100a,
+    on the same points with the same flush."""
+    mesh = n2w.Mesh.bumpy_sphere_trig(128, 256, 0.08, 6, 8)
+    mesh.normalize()
+    bvh = n2w.Bvh(mesh, 4, "sah")
+    pts = np.random.default_rng(12345).uniform(-1.2, 1.2, (n, 3)).astype(np.float32)
+    counted = bvh.query(pts, counted=True)
+    visits = float(counted["node_visits"].astype(np.int64).sum())
+    tests = float(counted["tri_tests"].astype(np.int64).sum())
+    dp = n2w.DeviceBuffer.from_array(pts, stream)
+    dd, dc, di, do = (n2w.DeviceBuffer(4 * n), n2w.DeviceBuffer(12 * n), n2w.DeviceBuffer(4 * n),
+                      n2w.DeviceBuffer(4 * n))
+
+    def timed(launch):
+        for _ in range(3):
+            launch()
+        stream.sync()
+        ms = []
+        for _ in range(repeat):
+            flush.zero(stream)
+            timer.start(stream)
+            launch()
+            timer.stop(stream)
+            ms.append(timer.ms())
+        return ms
+
+    ms = timed(lambda: bvh.query_device(dp.ptr, n, dd.ptr, dc.ptr, di.ptr, do.ptr, 128, stream))
+    d2 = dd.download(np.float32, n, stream)
+    ids = di.download(np.int32, n, stream)
+    ref = mesh.closest_point_host(pts[:validate])
+    bytes_q = n * (12 + 28) + visits * 128.0 + tests * 48.0
+    med = float(np.median(ms))
+    achieved = bytes_q / (med / 1e3) / 1e9
+    hbm, hbm_kind = peaks()
+    seg = {"workload": f"{n:,} queries uniform in [-1.2,1.2]^3 (PCG64 seed 12345), bumpy sphere "
+                       "r=1+0.08 sin6t cos8p 128x256 normalised (65,024 triangles), 4-wide SAH BVH leaf<=4, "
+                       "L2 flushed before every timed launch",
+           "queries_per_s": n / (med / 1e3), "kernel_ms_median": med, "kernel_ms_min": float(np.min(ms)),
+           "per_query": {"node_visits": visits / n, "tri_tests": tests / n, "algorithmic_bytes": bytes_q / n},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                        "peak_source": hbm_kind, "fractions": fractions(achieved, hbm, cache_peaks),
+                        "kernel": "closest_point_kernel"},
+           "validation": {"checked": validate,
+                          "triangle_id_mismatch": int(np.sum(ids[:validate] != ref["triangle_id"])),
+                          "distance2_mismatch": int(np.sum(d2[:validate] != ref["distance2"]))},
+           "gpu_launches": repeat}
+    if reference_kernel:
+        seg["reference_kernel"] = reference_kernel_leg(mesh, pts, dp, d2, stream, timed)
+        rk = seg["reference_kernel"]
+        if rk.get("queries_per_s"):
+            seg["speedup_vs_reference_kernel"] = seg["queries_per_s"] / rk["queries_per_s"]
+    return seg
+
+
+def reference_kernel_leg(mesh, pts, dp, d2_ours, stream, timed):
+    """Baseline leg: the reference's closest_point_bvh_kernel through its own
+    CudaBvh::query_device (oracle/_ref/libn2wos_ref_gpu.so, built from
+    src/cuda/bvh_query.cu + bvh_build_host.cpp), same device points."""
+    import oracle
+
+    if not oracle.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libn2wos_ref_gpu.so not built"}
+    import n2w
+
+    R = oracle.ref_gpu()
+    v, t = mesh.arrays()
+    h = R.ref_gpu_bvh_create(v.ctypes.data, len(v), t.ctypes.data, len(t), 8)
+    if not h:
+        return {"unavailable": R.ref_gpu_last_error().decode()}
+    n = len(pts)
+    dd, dc, di, do = (n2w.DeviceBuffer(4 * n), n2w.DeviceBuffer(12 * n), n2w.DeviceBuffer(4 * n),
+                      n2w.DeviceBuffer(4 * n))
+    try:
+        def launch():
+            if R.ref_gpu_query_device(h, dp.ptr, n, dd.ptr, dc.ptr, di.ptr, do.ptr, 128, stream.handle) != 0:
+                raise RuntimeError(R.ref_gpu_last_error().decode())
+        ms = timed(launch)
+        d2 = dd.download(np.float32, n, stream)
+        ov = int(do.download(np.int32, n, stream).sum())
+    finally:
+        R.ref_gpu_bvh_destroy(h)
+    med = float(np.median(ms))
+    return {"kernel": "closest_point_bvh_kernel (reference src/cuda/bvh_query.cu:75-160), median-split BVH leaf 8, "
+                      "block 128, compiled from its sources for sm_100a",
+            "queries_per_s": n / (med / 1e3), "kernel_ms_median": med, "overflow": ov,
+            "distance2_equal_to_ours": int(np.sum(d2 == d2_ours)), "queries": n}
+
+
+def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub=16384, train_steps=200,
+                real_stride=4, real_cap_s=60.0):
     """Time for the slice MSE against the FP64 analytic u to reach `target`:
-    plain GPU WoS vs NC+2LMC (cache trained online from WoS labels, coarse walks
-    truncated at depth m and closed by the cache, unbiased residual from fewer
-    walks continued to the boundary).  Per-walk cost and variance are measured
-    on the device for an evenly spaced subsample of the slice; MSE(N) = var / N
-    (both estimators are unbiased up to the epsilon shell) is extrapolated to
-    the full slice.
+    this project's plain GPU WoS against NC+2LMC (cache trained online from WoS
+    labels; coarse walks truncated at depth m and closed by the cache; the
+    unbiased residual level continues fewer walks to the boundary).
 
-    Reported: plain WoS with one and with 16 Green's-function source samples
-    per ball; NC+2LMC with 16 source samples at the configured depth 8 with
-    1/16 residual walks and at depth 1 with the optimal residual fraction; and
-    the bound any unbiased two-level correction obeys: the residual carries
-    Var(W | X_m) at full-walk cost, so the speedup over plain WoS with the same
-    walks is at most Var(W) / E[Var(W | X_m)] = 1 / (1 - R^2_m)."""
+    (1) Per-walk cost (CUDA events) and variance on an evenly spaced subsample
+        of the slice, for plain WoS with 1 and with 16 Green's-function source
+        samples per ball, and for NC+2LMC (16 samples) at depths 1, 2, 4, 8
+        with the trained cache and with the exact solution in place of the
+        cache.  With cost c and variance V per walk at each level, the best
+        allocation reaches MSE e in (sqrt(Vc cc) + sqrt(Vr cr))^2 / e per point.
+        The exact-solution column is the bound for any cache: the residual
+        level then carries E[Var(W | X_m)] at full-walk cost.
+    (2) Measured: on every `real_stride`-th slice point, walk blocks are added
+        until the measured MSE against the FP64 solution is below `target`:
+        plain WoS with 16 source samples, and NC+2LMC at the trained cache's
+        best depth with its optimal residual fraction (training time
+        included).  Times are CUDA-event sums over the blocks, scaled by
+        `real_stride` to the full slice (the cost is linear in the points; the
+        MSE is a mean over points, which the subsample estimates)."""
     from n2w import nc
 
     P = len(pts)
@@ -196,12 +362,14 @@ def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub
             ms = t.ms()
         r = st.download()
         tw, var = ms / 1e3 / (n * W), float(np.mean(r["sample_variance"]))
-        return {"s_per_walk": tw, "var_per_walk": var, "seconds": nc.time_to_mse(target, P * tw, var, 0.0)}
+        return {"s_per_walk": tw, "var_per_walk": var, "seconds_extrapolated": nc.time_to_mse(target, P * tw, var, 0.0)}
 
     out["plain_wos"] = plain(problem)
     p16 = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
     p16.source_samples = 16
     out["plain_wos_16_source_samples"] = plain(p16)
+    var16 = out["plain_wos_16_source_samples"]["var_per_walk"]
+    t16 = out["plain_wos_16_source_samples"]["s_per_walk"]
 
     cache = n2w.Cache(n2w.cache_config())
     t.start()
@@ -209,40 +377,118 @@ def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub
     t.stop()
     train_s = t.ms() / 1e3
 
-    def level(m, coarse, resid):
+    def level(c, m, coarse, resid):
         o = nc.nc2lmc_options(mesh, coarse_walks=coarse, residual_walks=resid, depth_m=m, epsilon=5e-4, seed=7)
         ms, r = [], None
         for _ in range(3):  # best of three (the first includes one-time scratch mapping)
             t.start()
-            r = nc.nc2lmc(bvh, p16, cache, x, o, d_points=dp)
+            r = nc.nc2lmc(bvh, p16, c, x, o, d_points=dp)
             t.stop()
             ms.append(t.ms())
         return min(ms) / 1e3 / (n * max(coarse, resid)), r
 
-    var16 = out["plain_wos_16_source_samples"]["var_per_walk"]
-    for m in (8, 1):
-        tc, rc = level(m, W, 0)
-        tr, rr = level(m, 0, W)
-        vc = float(np.mean(rc["coarse"]["sample_variance"]))
-        vr = float(np.mean(rr["residual"]["sample_variance"]))
-        spec = nc.time_to_mse(target, P * (tc + tr / 16), vc + 16 * vr, 0.0, train_s)  # Nr = Nc / 16
-        opt = train_s + P * (np.sqrt(vc * tc) + np.sqrt(vr * tr)) ** 2 / target
-        out[f"nc2lmc_m{m}"] = {"depth_m": m, "s_per_coarse_walk": tc, "s_per_residual_walk": tr, "var_coarse": vc,
-                               "var_residual": vr, "seconds_residual_1_16": spec, "seconds_optimal_allocation": opt,
-                               "optimal_residual_fraction": float(np.sqrt((vr / tr) / (vc / tc))),
-                               "explained_variance_R2": max(0.0, 1.0 - vr / var16),
-                               "speedup_bound_vs_same_walks": var16 / vr}
-    best = min(out["nc2lmc_m8"]["seconds_optimal_allocation"], out["nc2lmc_m1"]["seconds_optimal_allocation"])
+    levels = {}
+    for cache_kind, c in (("trained", cache), ("exact_solution", None)):
+        for m in (1, 2, 4, 8):
+            tc, rc = level(c, m, W, 0)
+            tr, rr = level(c, m, 0, W)
+            vc = float(np.mean(rc["coarse"]["sample_variance"]))
+            vr = float(np.mean(rr["residual"]["sample_variance"]))
+            fixed = train_s if c is not None else 0.0
+            opt = fixed + P * (np.sqrt(vc * tc) + np.sqrt(vr * tr)) ** 2 / target
+            levels[f"{cache_kind}_m{m}"] = {
+                "cache": cache_kind, "depth_m": m, "s_per_coarse_walk": tc, "s_per_residual_walk": tr,
+                "var_coarse": vc, "var_residual": vr, "seconds_optimal_allocation": opt,
+                "seconds_residual_1_16": nc.time_to_mse(target, P * (tc + tr / 16), vc + 16 * vr, 0.0, fixed),
+                "optimal_residual_fraction": float(np.sqrt((vr / tr) / (vc / tc))),
+                "explained_variance_R2": max(0.0, 1.0 - vr / var16),
+                "speedup_vs_plain_16_same_walks": (P * var16 * t16 / target) / opt}
+    out["nc2lmc_levels"] = levels
+    trained = {k: v for k, v in levels.items() if v["cache"] == "trained"}
+    bound = {k: v for k, v in levels.items() if v["cache"] == "exact_solution"}
+    best = min(trained.values(), key=lambda v: v["seconds_optimal_allocation"])
+    best_bound = min(bound.values(), key=lambda v: v["seconds_optimal_allocation"])
     out["nc2lmc_training"] = {"train_s": train_s, "train_steps": train_steps, "train_batch": 65536,
                               "walks_per_label": 32, "source_samples": 16,
                               "loss_first_last": [float(losses[0]), float(losses[-1])]}
-    out["speedup_nc2lmc_vs_plain"] = out["plain_wos"]["seconds"] / best
-    out["speedup_nc2lmc_vs_plain_16_source_samples"] = out["plain_wos_16_source_samples"]["seconds"] / best
-    out["speedup_nc2lmc_config2_vs_plain"] = out["plain_wos"]["seconds"] / out["nc2lmc_m8"]["seconds_residual_1_16"]
-    out["method"] = ("per-walk cost by CUDA events and per-walk variance on a subsample; "
-                     "MSE(N) = var/N extrapolated to the full slice; training time included")
+    out["extrapolated"] = {
+        "speedup_nc2lmc_vs_plain_16_source_samples": out["plain_wos_16_source_samples"]["seconds_extrapolated"] /
+        best["seconds_optimal_allocation"],
+        "best_trained_depth": best["depth_m"],
+        "bound_exact_solution_cache_speedup": best_bound["speedup_vs_plain_16_same_walks"],
+        "bound_depth": best_bound["depth_m"],
+        "config2_m8_residual_1_16_speedup_vs_plain_16": out["plain_wos_16_source_samples"]["seconds_extrapolated"] /
+        levels["trained_m8"]["seconds_residual_1_16"],
+        "one_sample_plain_vs_nc2lmc_16_samples_not_like_for_like": out["plain_wos"]["seconds_extrapolated"] /
+        best["seconds_optimal_allocation"]}
+    out["measured"] = measured_time_to_mse(n2w, call, bvh, mesh, pts, exact, p16, cache, best, train_s, target,
+                                           real_stride, real_cap_s)
+    m = out["measured"]
+    if m["plain_16"].get("reached") and m["nc2lmc"].get("reached"):
+        out["speedup_nc2lmc_vs_plain_16_source_samples"] = m["plain_16"]["seconds_full_slice"] / \
+            m["nc2lmc"]["seconds_full_slice"]
     out["progressive_snapshots"] = progressive_overlap(n2w, mesh, bvh, pts, p16)
     return out
+
+
+def measured_time_to_mse(n2w, call, bvh, mesh, pts, exact, problem, cache, best, train_s, target, stride, cap_s):
+    """Adds walk blocks until the slice MSE against the FP64 solution is below
+    `target` on every `stride`-th slice point (see time_to_mse)."""
+    from n2w import nc
+
+    x = np.ascontiguousarray(pts[::stride])
+    ex = exact[::stride]
+    n = len(x)
+    dp = n2w.DeviceBuffer.from_array(x)
+    t = n2w.Timer()
+    res = {"points": n, "stride": stride, "target_mse": target, "cap_seconds_subsample": cap_s}
+
+    # plain WoS, 16 source samples, blocks of 512 walks per point accumulated on the device
+    st = n2w.PointStatsBuffers.allocate(n)
+    ws = n2w.DeviceBuffer(n2w._lib.lib.n2w_wos_workspace_bytes(n))
+    total_ms, blocks, mse = 0.0, 0, None
+    while total_ms / 1e3 < cap_s:
+        o = n2w.walk_options(walks_per_point=512, epsilon=5e-4, seed=1000 + blocks, accumulate=1 if blocks else 0)
+        t.start()
+        call("n2w_wos_estimate", bvh.handle, C.byref(problem), dp.ptr, n, C.byref(o), st.struct(), None, ws.ptr, None)
+        t.stop()
+        total_ms += t.ms()
+        blocks += 1
+        r = st.download()
+        mse = float(np.mean((r["mean"] - ex) ** 2))
+        if mse < target:
+            break
+    res["plain_16"] = {"reached": bool(mse is not None and mse < target), "mse": mse, "blocks": blocks,
+                       "walks_per_point": 512 * blocks, "seconds_subsample": total_ms / 1e3,
+                       "seconds_full_slice": total_ms / 1e3 * stride}
+
+    # NC+2LMC at the trained cache's best depth with its optimal residual fraction
+    m = best["depth_m"]
+    frac = min(1.0, max(best["optimal_residual_fraction"], 1.0 / 64))
+    wc = 256
+    wr = max(1, int(round(wc * frac)))
+    acc = {k: [np.zeros(n), np.zeros(n), np.zeros(n)] for k in ("c", "r")}
+    total_ms, blocks, mse = 0.0, 0, None
+    while total_ms / 1e3 + train_s / stride < cap_s:
+        o = nc.nc2lmc_options(mesh, coarse_walks=wc, residual_walks=wr, depth_m=m, epsilon=5e-4, seed=5000 + blocks)
+        t.start()
+        r = nc.nc2lmc(bvh, problem, cache, x, o, d_points=dp)
+        t.stop()
+        total_ms += t.ms()
+        blocks += 1
+        for k, lv in (("c", r["coarse"]), ("r", r["residual"])):
+            acc[k][0] += lv["sum"]
+            acc[k][1] += lv["sum_sq"]
+            acc[k][2] += lv["count"]
+        est = acc["c"][0] / acc["c"][2] + acc["r"][0] / acc["r"][2]
+        mse = float(np.mean((est - ex) ** 2))
+        if mse < target:
+            break
+    res["nc2lmc"] = {"reached": bool(mse is not None and mse < target), "mse": mse, "blocks": blocks,
+                     "depth_m": m, "coarse_walks_per_point": wc * blocks, "residual_walks_per_point": wr * blocks,
+                     "seconds_subsample_walks": total_ms / 1e3, "train_seconds": train_s,
+                     "seconds_full_slice": total_ms / 1e3 * stride + train_s}
+    return res
 
 
 def progressive_overlap(n2w, mesh, bvh, pts, problem, blocks=4, train_steps=12):
@@ -275,42 +521,156 @@ def progressive_overlap(n2w, mesh, bvh, pts, problem, blocks=4, train_steps=12):
 
 
 def run_reference(args):
-    import n2w
-
+    """The reference path's CPU implementation on this arm's workload (rank 0
+    only): the headline slice rebuilt by the oracle and the reference's own
+    sources (no product code), each step a fixed sample of it (every
+    REF_SAMPLE_STRIDE-th interior point x 1,024 walks, a new walk stream per step)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from n2w._lib import call, lib  # noqa: F401 (host-only use: mesh, host BVH layout)
-
-    mesh = n2w.Mesh.icosphere_displaced(6, 0.12, 3.0, 4, 0.5, 12345)
-    mesh.normalize()
-    host = n2w.HostBvh(mesh, 4, "sah")
-    layout = host.layout()
-    lo, hi = mesh.bounds()
-    grid, _ = n2w.slice_points(lo, hi, "xy", 0.12, 512, 512, 0.02, True)
-    import oracle
-
-    v, t = mesh.arrays()
-    # interior mask with the reference rule on a strided subset (CPU brute force is O(points x tris))
-    cand = grid[::97]
-    inside = oracle.inside_bruteforce(v, t, cand).astype(bool)
-    pts = np.ascontiguousarray(cand[inside])
-    problem = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
+    try:
+        scene = reference_cpu_scene()
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return 0
     vals = []
     for i in range(args.warmup + args.steps):
-        s = cpu_port_sample(n2w, layout, problem, pts, 1024, seconds_target=8.0)
+        s = reference_cpu_sample(scene, 1024, seed=12345 + i)
         if i >= args.warmup:
             vals.append(s)
-    value = float(np.mean([s["value"] for s in vals]))
+    steps_per_s = [s["value"] for s in vals]
+    value = float(np.mean(steps_per_s))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
-            "data": "synthetic", "config": CONFIG,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, points=int(len(scene[1]))),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[-1]["cores"], "kind": "port",
                              "sample": vals[-1]["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "reference walker is GPU-only (cuBQL, not vendored); CPU path = oracle port of "
-                    "nc_wos_from_point (src/cuda/cubql_bvh.cu:1323-1357) over a CPU BVH, all host threads"}
+            "step_values": steps_per_s,
+            "libraries_loaded": loaded_libraries(),
+            "note": "the reference's walker exists only as GPU code on cuBQL (not vendored); its CPU form here is "
+                    "the oracle's port of nc_wos_from_point over the reference's own median-split host BVH "
+                    "(oracle/_ref, built from its sources), on every host thread; no product code is loaded"}
     print(json.dumps(line))
+    return 0
+
+
+def run_figure(args):
+    """The reference's two published evaluation runs (figures/zebra_k8_m2.json,
+    figures/bunny_zebra_k8_m2.json: RTX 3070, cuBQL, tiny-cuda-nn), re-run with
+    their exact command lines through this project's n2wos_eval_tcnn_nc_wos
+    (output paths redirected; the bunny PLY from the copy staged under
+    oracle/_ref).  Reported per run: pure-WoS walk-steps/s (samples x mean steps
+    / CUDA-event time) against the published figure, and the published vs
+    measured mesh, mask and estimator statistics."""
+    import shutil
+
+    golden = json.loads((ROOT / "tests" / "golden" / "figure_runs.json").read_text())
+    tool = ROOT / "n2wos-cuda_b200" / "bin" / "n2wos_eval_tcnn_nc_wos"
+    bunny = ROOT / "oracle" / "_ref" / "meshes" / "bunny_zipper_wataertight.ply"
+    out_dir = Path(tempfile.mkdtemp(prefix="n2w_figure_"))
+    runs = {}
+    try:
+        for name, fig in sorted(golden.items()):
+            argv = fig["command_line"].split()[1:]
+            fixed, i = [], 0
+            while i < len(argv):
+                a = argv[i]
+                if a in ("--mesh-path", "--save-estimates-prefix", "--output"):
+                    val = {"--mesh-path": str(bunny), "--save-estimates-prefix": str(out_dir / name),
+                           "--output": str(out_dir / f"{name}.json")}[a]
+                    fixed += [a, val]
+                    i += 2
+                else:
+                    fixed.append(a)
+                    i += 1
+            r = subprocess.run([str(tool), *fixed], capture_output=True, text=True, timeout=1200)
+            if r.returncode != 0:
+                runs[name] = {"error": r.stderr[-2000:]}
+                continue
+            js = json.loads((out_dir / f"{name}.json").read_text())
+            got, want = js["runs"]["pure_wos"], fig["runs"]["pure_wos"]
+            ws = got["samples"] * got["mean_steps"] / (got["elapsed_ms"] / 1e3)
+            ws_pub = want["samples"] * want["mean_steps"] / (want["elapsed_ms"] / 1e3)
+            runs[name] = {
+                "walk_steps_per_s": ws, "published_walk_steps_per_s": ws_pub, "published_device": fig["device"],
+                "speedup_vs_published": ws / ws_pub,
+                "eval_points": [got["eval_points"], want["eval_points"]],
+                "mean_steps": [got["mean_steps"], want["mean_steps"]],
+                "mean_sample_variance": [got["mean_sample_variance"], want["mean_sample_variance"]],
+                "rmse": [got["rmse"], want["rmse"]], "elapsed_ms": [got["elapsed_ms"], want["elapsed_ms"]],
+                "mesh_triangles": [js["mesh_stats"]["triangles"], fig["mesh_stats"]["triangles"]],
+                "normalization": [js["mesh_stats"]["normalization"], fig["mesh_stats"]["normalization"]],
+                "nc_wos_rmse": [js["runs"]["nc_wos"]["rmse"], fig["runs"]["nc_wos"]["rmse"]],
+                "nc_2lmc_rmse": [js["runs"]["nc_2lmc"]["rmse"], fig["runs"]["nc_2lmc"]["rmse"]],
+                "training_ms": [js["training"]["total_training_ms"], fig["training"]["total_training_ms"]],
+                "pairs": "[this run, published]"}
+    finally:
+        shutil.rmtree(out_dir, ignore_errors=True)
+    head = runs.get("zebra_k8_m2", {})
+    line = {"metric": "walk-steps/s (pure WoS, reference figure run zebra_k8_m2: bumpy sphere 65,024 tris, "
+                      "harmonic_zebra_k8, z=0 slice 512x512 = 162,215 px x 64 walks, eps=1e-4)",
+            "value": head.get("walk_steps_per_s"), "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (the reference's own procedural mesh and "
+            "bundled bunny, its published command lines)",
+            "vs_baseline": head.get("speedup_vs_published"),
+            "config": {"workload": "reference figure runs zebra_k8_m2 and bunny_zebra_k8_m2, exact command lines"},
+            "runs": runs}
+    print(json.dumps(line))
+    return 0
+
+
+def run_nc_levels(args):
+    """Cost of the NC+2LMC levels, one call each: the headline slice's points
+    (--nc-points of them, evenly spaced), the sin-product
+    problem with 16 Green's-function source samples per ball, eps = 5e-4; the
+    default cache trained for --nc-train-steps steps of 65,536 points x 32-walk
+    labels; then the coarse level alone (walks truncated at --nc-depth and closed
+    by the cache) and the residual level alone, each once untimed and once timed
+    with CUDA events.  Under a launch-list profiler the kernels of each call show
+    how a level's time splits between walks and cache inference."""
+    import n2w
+    from n2w import nc
+    from n2w._lib import call, lib
+
+    call("n2w_set_device", int(os.environ.get("LOCAL_RANK", "0")))
+    mesh, bvh, pts, _, _, _ = build_scene(n2w, lib, call)
+    x = np.ascontiguousarray(pts[np.linspace(0, len(pts) - 1, min(args.nc_points, len(pts))).astype(np.int64)])
+    n = len(x)
+    problem = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
+    problem.source_samples = 16
+    cache = n2w.Cache(n2w.cache_config())
+    nc.train(cache, bvh, problem, mesh, steps=args.nc_train_steps, batch=65536, walks_per_label=32, epsilon=5e-4)
+    dp = n2w.DeviceBuffer.from_array(x)
+    timer = n2w.Timer()
+    W = args.walks if args.walks != 1024 else 256
+    out = {"workload": "nc-levels", "points": n, "walks_per_point": W, "depth_m": args.nc_depth,
+           "train_steps": args.nc_train_steps, "samples_per_call": n * W}
+    for name, coarse, resid in (("coarse", W, 0), ("residual", 0, W)):
+        o = nc.nc2lmc_options(mesh, coarse_walks=coarse, residual_walks=resid, depth_m=args.nc_depth, epsilon=5e-4,
+                              seed=7)
+        nc.nc2lmc(bvh, problem, cache, x, o, d_points=dp)  # untimed: one-time scratch mapping
+        timer.start()
+        r = nc.nc2lmc(bvh, problem, cache, x, o, d_points=dp)
+        timer.stop()
+        level = r["coarse"] if coarse else r["residual"]
+        out[name] = {"ms_per_call": timer.ms(), "s_per_walk": timer.ms() / 1e3 / (n * W),
+                     "var_per_walk": float(np.mean(level["sample_variance"]))}
+    print(json.dumps(out))
+    return 0
+
+
+def run_query(args):
+    """The config-0 closest-point segment of the default line on its own, with
+    --queries points (the default 262,144 is config 0)."""
+    import n2w
+    from n2w._lib import call
+
+    call("n2w_set_device", int(os.environ.get("LOCAL_RANK", "0")))
+    stream = n2w.Stream()
+    seg = closest_point_segment(n2w, call, stream, n2w.Timer(), n2w.DeviceBuffer(256 << 20), cache_level_peaks(call),
+                                reference_kernel=not args.no_reference_kernel, n=args.queries)
+    print(json.dumps(dict(metric="closest-point queries/s", value=seg["queries_per_s"], unit="queries/s", **seg)))
     return 0
 
 
@@ -458,6 +818,11 @@ def run_batch(args):
 
 
 def run_serve(args):
+    print(json.dumps(serve_line(args)))
+    return 0
+
+
+def serve_line(args):
     """Serving loop under mixed load: Poisson arrivals of requests on 4
     device-resident meshes (the config-0 bumpy sphere, the config-1 icosphere,
     the smallest and largest config-3 spheres) with either an 8-charge harmonic
@@ -629,8 +994,7 @@ def run_serve(args):
         # inference, combine and reduction, plus the chunk's add (more when a chunk splits into batches)
         "gpu_launches": int(st["ticks"]) * 2 + int(st["nc_chunks"]) * 11,
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def main():
@@ -645,9 +1009,10 @@ def main():
     ap.add_argument("--points", type=int, default=0,
                     help="use only the first N slice points (smaller workload for profiler captures; "
                          "the default 0 runs the full slice)")
-    ap.add_argument("--workload", default="slice", choices=["slice", "batch", "serve"],
+    ap.add_argument("--workload", default="slice", choices=["slice", "batch", "serve", "figure", "nc-levels", "query"],
                     help="slice: the headline Poisson slice (default); batch: 64 batched Laplace instances; "
-                         "serve: the serving loop under Poisson arrivals")
+                         "serve: the serving loop under Poisson arrivals; figure: the reference's published "
+                         "figure runs; nc-levels: one call of each NC+2LMC level (for launch-list profiles)")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-rate", type=float, default=10.0, help="mean arrivals per second")
     ap.add_argument("--serve-large-fraction", type=float, default=0.05)
@@ -665,6 +1030,21 @@ def main():
     ap.add_argument("--serve-nc-fraction", type=float, default=0.1,
                     help="fraction of requests served as NC+2LMC with a pre-trained cache")
     ap.add_argument("--serve-nc-train-steps", type=int, default=200)
+    ap.add_argument("--e2e-steps", type=int, default=5, help="end-to-end steps (host buffers) timed after the "
+                    "device-resident ones (at most --steps)")
+    ap.add_argument("--no-closest-point", action="store_true", help="skip the config-0 closest-point segment")
+    ap.add_argument("--no-serve", action="store_true", help="skip the short serving segment of the default line")
+    ap.add_argument("--line-serve-requests", type=int, default=200,
+                    help="requests of the default line's serving segment (Poisson arrivals at --serve-rate)")
+    ap.add_argument("--line-serve-time-limit", type=float, default=45.0)
+    ap.add_argument("--nc-points", type=int, default=16384, help="nc-levels: evenly spaced slice points")
+    ap.add_argument("--nc-depth", type=int, default=1, help="nc-levels: truncation depth m")
+    ap.add_argument("--nc-train-steps", type=int, default=5, help="nc-levels: training steps before the calls")
+    ap.add_argument("--queries", type=int, default=262144, help="query: number of uniform query points")
+    ap.add_argument("--no-reference-kernel", action="store_true",
+                    help="query / default line: skip the reference closest-point kernel baseline leg")
+    ap.add_argument("--ttm-stride", type=int, default=4,
+                    help="the measured time-to-MSE runs use every N-th slice point, scaled to the full slice")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -672,6 +1052,12 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "figure":
+        return run_figure(args)
+    if args.workload == "nc-levels":
+        return run_nc_levels(args)
+    if args.workload == "query":
+        return run_query(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -767,7 +1153,7 @@ def main():
     call("n2w_malloc_host", C.byref(hout), out_bytes)
     e2e_times = []
     barrier()
-    for i in range(max(1, args.steps)):
+    for i in range(max(1, min(args.steps, args.e2e_steps))):
         flush.zero(stream)
         timer.start(stream)
         call("n2w_memcpy_h2d", d_pts.ptr, hp, pts.nbytes, stream.handle)
@@ -796,19 +1182,35 @@ def main():
     alg_bytes = c_last["node_visits"] * 128.0 + c_last["tri_tests"] * 48.0 + n * (12 + 8 + 8 + 4 + 8 + 4)
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
+    cache_peaks = cache_level_peaks(call)
 
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             try:
-                cpu = cpu_port_sample(n2w, bvh.layout(), problem, pts, W)
+                ref_scene = reference_cpu_scene()
+                cpu = reference_cpu_sample(ref_scene, W)
+                cpu["same_points_as_gpu_workload"] = bool(args.points == 0 and np.array_equal(ref_scene[1], pts))
             except Exception as e:  # the baseline must never break the bench line
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                        "sample": f"failed: {e}"}
         wsteps_per_walk = c_last["steps"] / max(c_last["walks"], 1)
+        cp_seg = None
+        if not args.no_closest_point and world == 1:
+            cp_seg = closest_point_segment(n2w, call, stream, timer, flush, cache_peaks,
+                                           reference_kernel=not args.no_reference_kernel)
         ttm = None
         if not args.no_ttm and world == 1 and args.points == 0:
-            ttm = time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem)
+            ttm = time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, real_stride=args.ttm_stride)
+        serving = None
+        if not args.no_serve and world == 1 and args.points == 0:
+            sargs = argparse.Namespace(**vars(args))
+            sargs.serve_requests, sargs.serve_time_limit = args.line_serve_requests, args.line_serve_time_limit
+            sargs.serve_nc_train_steps = 50
+            serving = serve_line(sargs)
+            serving = {k: serving[k] for k in ("metric", "value", "unit", "config", "complete", "finished_requests",
+                                                "latency_s", "throughput", "accuracy", "modes", "clocks",
+                                                "gpu_launches") if k in serving}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -824,13 +1226,19 @@ def main():
                          "traffic_source": "profiles/walker_kernel_icosphere_slice_4096pts.md (scaled by walk-steps)",
                          "peak_source": peak_kind,
                          "kernel": "walker_kernel", "bytes_per_launch": alg_bytes,
-                         "kernel_ms": kernel_ms},
+                         "kernel_ms": kernel_ms, "fractions": fractions(achieved, peak, cache_peaks),
+                         "cache_level_peaks_gbs": cache_peaks,
+                         "note": "algorithmic bytes are L1/L2 hits (BVH + triangles L2-resident); frac is the "
+                                 "HBM-copy scale, fractions.l1 / fractions.l2 divide by this box's measured L1 / L2 "
+                                 "read bandwidth"},
             "cpu_baseline": cpu,
             "gpu_launches": 2 * args.steps,  # per step: first-query pre-pass + persistent walker
             "clocks": clocks.summary(),
             "accuracy": {"mse_vs_fp64_exact": mse, "mean_estimator_variance": var_part, "bias2_estimate": bias2,
                          "walks_per_point": W * world, "mean_steps_per_walk": wsteps_per_walk},
             "time_to_mse_1e-4": ttm,
+            "closest_point": cp_seg,
+            "serving": serving,
             "counters_last_step": c_last,
             "walks_per_s": c_last["walks"] / (kernel_ms / 1e3),
         }

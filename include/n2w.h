@@ -767,6 +767,13 @@ int n2w_timer_elapsed_ms(n2w_timer* t, float* ms_out); /* synchronises on the st
 void n2w_timer_destroy(n2w_timer* t);
 int n2w_sm_count(int* out);
 int n2w_mem_info(size_t* free_bytes, size_t* total_bytes);
+/* Sustained read bandwidth (GB/s) of one on-chip level, measured by the
+ * library's own probe kernels on the current device: level 1 = each block
+ * re-reads its own 16 KiB slice (L1 hits), level 2 = a `bytes` buffer that fits
+ * in L2 streamed with loads that bypass L1.  The roofline denominator for the
+ * L1/L2-resident traversal.  Allocates its buffers.  No counterpart in the
+ * reference. */
+int n2w_probe_read_bandwidth(int level, size_t bytes, int iterations, double* gbs_out);
 
 #ifdef __cplusplus
 }  /* extern "C" */

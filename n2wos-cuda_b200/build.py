@@ -33,7 +33,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{CUDA_HOME / 'include'}"]
 
-LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu", "util.cu", "batch.cu", "server.cu"]
+LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu", "util.cu", "batch.cu", "server.cu", "probe.cu"]
 LIB_CPP = ["mesh.cpp", "bvh_build.cpp", "capi.cpp"]
 EXECUTABLES = {
     "n2wos_probe_cuda_bvh": ["probe_cuda_bvh.cpp"],

@@ -294,6 +294,7 @@ _SIGS = {
     "n2w_timer_destroy": (None, [P]),
     "n2w_sm_count": (I, [C.POINTER(I)]),
     "n2w_mem_info": (I, [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "n2w_probe_read_bandwidth": (I, [I, C.c_size_t, I, C.POINTER(C.c_double)]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -59,7 +59,9 @@ def nc2lmc_options(mesh, coarse_walks=256, residual_walks=16, depth_m=8, max_ste
 
 def nc2lmc(bvh, problem, cache, points, options, stream=None, d_points=None):
     """Runs coarse + residual levels; returns per-point combined estimate,
-    estimator variance and the per-level statistics."""
+    estimator variance and the per-level statistics.  cache=None closes the
+    coarse walks with the exact solution instead of a network (the analytic
+    stand-in: the best any cache can do, used for bounds)."""
     if d_points is None:
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         n = len(pts)
@@ -68,8 +70,12 @@ def nc2lmc(bvh, problem, cache, points, options, stream=None, d_points=None):
         n = len(points)
     cs, rs = PointStatsBuffers.allocate(n), PointStatsBuffers.allocate(n)
     s = stream.handle if stream else None
-    call("n2w_nc2lmc_estimate", bvh.handle, C.byref(problem), cache.handle, d_points.ptr, n, C.byref(options),
-         cs.struct(), rs.struct(), s)
+    if cache is None:
+        call("n2w_nc2lmc_estimate_ex", bvh.handle, C.byref(problem), None, d_points.ptr, n, C.byref(options),
+             cs.struct(), rs.struct(), None, s)
+    else:
+        call("n2w_nc2lmc_estimate", bvh.handle, C.byref(problem), cache.handle, d_points.ptr, n, C.byref(options),
+             cs.struct(), rs.struct(), s)
     call("n2w_stream_sync", s)
     c = cs.download(stream) if options.coarse_walks > 0 else None
     r = rs.download(stream) if options.residual_walks > 0 else None

@@ -436,3 +436,21 @@ def slice_points(bounds6, view="xy", plane=0.0, width=512, height=512, padding=0
                              int(preserve_aspect), rule, _p(pts), _p(frame)) != 0:
         raise ValueError("bad slice view")
     return pts, frame
+
+
+def problem_record(mode, source_sampling=0, omega=0.0, source_samples=0, charges=None) -> bytes:
+    """A boundary-problem record with the byte layout the walkers read (mode,
+    source rule, charge count, omega, 16 x (x, y, z, amplitude) charges, source
+    samples per ball, reserved).  Modes the oracle evaluates: 0 (x^2 - y^2),
+    4 (Re((x + i y)^8)), 12 (constant 1), 100 (charges), 101 (sin product with
+    f = 3 omega^2 u)."""
+    import struct
+
+    ch = np.zeros((16, 4), np.float32)
+    count = 0
+    if charges is not None:
+        c = np.asarray(charges, np.float32).reshape(-1, 4)
+        count = len(c)
+        ch[:count] = c
+    return (struct.pack("<iiif", mode, source_sampling, count, np.float32(omega)) + ch.tobytes() +
+            struct.pack("<ii", source_samples, 0))
