@@ -818,7 +818,31 @@ def run_batch(args):
 
 
 def run_serve(args):
-    print(json.dumps(serve_line(args)))
+    if not args.serve_rates:
+        print(json.dumps(serve_line(args)))
+        return 0
+    # offered-load sweep: each rate runs --serve-sweep-seconds of Poisson arrivals
+    sweep = []
+    for rate in [float(r) for r in args.serve_rates.split(",")]:
+        a = argparse.Namespace(**vars(args))
+        a.serve_rate = rate
+        a.serve_requests = max(20, int(rate * args.serve_sweep_seconds))
+        a.serve_time_limit = args.serve_sweep_seconds + args.serve_sweep_drain
+        line = serve_line(a)
+        sweep.append({"offered_req_per_s": rate, "requests": a.serve_requests, "complete": line["complete"],
+                      "finished": line["finished_requests"], "latency_s": line["latency_s"],
+                      "throughput": line["throughput"], "accuracy": line["accuracy"],
+                      "nc2lmc": line["modes"]["nc2lmc"], "clocks": line["clocks"]})
+        print(f"[serve sweep] rate {rate}: p50 {line['latency_s']['p50']:.3f}s p99<=4096 "
+              f"{line['latency_s']['p99_le4096']:.3f}s done {line['finished_requests']}/{a.serve_requests}",
+              file=sys.stderr, flush=True)
+    sat = [r for r in sweep if not r["complete"] or r["latency_s"]["p99_le4096"] > 10 * sweep[0]["latency_s"]["p99_le4096"]]
+    print(json.dumps({"metric": "serving loop p50/p99 latency vs offered load", "value": None, "unit": "s",
+                      "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+                      "config": {"workload": "serving sweep (see --workload serve)", "rates": args.serve_rates,
+                                 "seconds_of_arrivals_per_rate": args.serve_sweep_seconds},
+                      "sweep": sweep,
+                      "first_saturated_rate": sat[0]["offered_req_per_s"] if sat else None}))
     return 0
 
 
@@ -1030,6 +1054,9 @@ def main():
     ap.add_argument("--serve-nc-fraction", type=float, default=0.1,
                     help="fraction of requests served as NC+2LMC with a pre-trained cache")
     ap.add_argument("--serve-nc-train-steps", type=int, default=200)
+    ap.add_argument("--serve-rates", default="", help="serve: comma-separated offered rates to sweep (req/s)")
+    ap.add_argument("--serve-sweep-seconds", type=float, default=30.0, help="serve sweep: seconds of arrivals per rate")
+    ap.add_argument("--serve-sweep-drain", type=float, default=30.0, help="serve sweep: extra seconds to drain")
     ap.add_argument("--e2e-steps", type=int, default=5, help="end-to-end steps (host buffers) timed after the "
                     "device-resident ones (at most --steps)")
     ap.add_argument("--no-closest-point", action="store_true", help="skip the config-0 closest-point segment")
@@ -1062,20 +1089,18 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     import n2w
     from n2w._lib import call, lib
 
     call("n2w_set_device", local)
+    comm = None
+    if world > 1:
+        # one process per GPU; NCCL through the library's C ABI, the id handed
+        # over by a file keyed by this launch (the ranks share their parent)
+        from n2w.shard import NcclComm
+
+        comm = NcclComm(rank, world, key=f"{os.environ.get('MASTER_PORT', '0')}_{os.getppid()}")
     mesh, bvh, pts, problem, exact, frame = build_scene(n2w, lib, call)
     if args.points > 0:
         sel = np.linspace(0, len(pts) - 1, min(args.points, len(pts))).astype(np.int64)
@@ -1097,8 +1122,8 @@ def main():
     timer = n2w.Timer()
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        if comm is not None:
+            comm.barrier()
 
     def step(o):
         call("n2w_wos_estimate", bvh.handle, C.byref(problem), d_pts.ptr, n, C.byref(o), stats.struct(),
@@ -1124,21 +1149,17 @@ def main():
         barrier()
     total_ms = float(np.sum(times))
     steps_done = float(sum(c["steps"] for c in counters))
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([total_ms, steps_done], dtype=torch.float64, device=f"cuda:{local}")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        total_ms, steps_done = float(tmax[0]), float(t[1])
+    if comm is not None:
+        total_ms = float(comm.allreduce_host([np.array([total_ms])], "max")[0][0])
+        steps_done = float(comm.allreduce_host([np.array([steps_done])], "sum")[0][0])
     value = steps_done / (total_ms / 1e3)
 
     # accuracy of the last step (per-point FP64 sums -> MSE vs FP64 analytic);
-    # with several ranks, the combined estimate of all ranks' walks
+    # with several ranks, the combined estimate of all ranks' walks (summed on
+    # the device over NCCL)
+    if comm is not None:
+        comm.allreduce_point_stats_device(stats, n, stream)
     res = stats.download(stream)
-    if dist is not None:
-        res = shard.allreduce_point_stats(res)
     err = res["mean"] - exact
     mse = float(np.mean(err ** 2))
     var_part = float(np.mean(res["stderr"] ** 2))
@@ -1166,14 +1187,9 @@ def main():
     barrier()
     e2e_ms = float(np.sum(e2e_times))
     e2e_steps = float(np.mean([c["steps"] for c in counters])) * len(e2e_times)
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([e2e_ms, e2e_steps], dtype=torch.float64, device=f"cuda:{local}")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        e2e_ms, e2e_steps = float(tmax[0]), float(t[1])
+    if comm is not None:
+        e2e_ms = float(comm.allreduce_host([np.array([e2e_ms])], "max")[0][0])
+        e2e_steps = float(comm.allreduce_host([np.array([e2e_steps])], "sum")[0][0])
     lib.n2w_free_host(hp)
     lib.n2w_free_host(hout)
 
@@ -1243,9 +1259,9 @@ def main():
             "walks_per_s": c_last["walks"] / (kernel_ms / 1e3),
         }
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    if comm is not None:
+        comm.barrier()
+        comm.close()
     return 0
 
 

@@ -47,6 +47,7 @@ typedef struct n2w_vec3 {
 
 typedef struct n2w_mesh n2w_mesh; /* host triangle mesh (opaque) */
 typedef struct n2w_bvh n2w_bvh;   /* device-resident BVH + triangles (opaque) */
+typedef struct n2w_comm n2w_comm; /* NCCL communicator of one rank (opaque) */
 
 const char* n2w_last_error(void);
 int n2w_abi_version(void);
@@ -386,6 +387,12 @@ int n2w_cache_gradients(n2w_cache* cache, const float* d_inputs, const float* d_
 int n2w_cache_train_step(n2w_cache* cache, const float* d_inputs, const float* d_targets, int64_t n,
                          float* h_loss_out, n2w_stream_t stream);
 int n2w_cache_zero_grad(n2w_cache* cache, n2w_stream_t stream);
+/* The cache's FP32 gradient buffer (count floats, [grid | mlp]) and its device
+ * loss sum, for callers that reduce gradients with their own communicator:
+ * n2w_cache_gradients -> reduce the buffer in place -> n2w_cache_apply_gradients. */
+int n2w_cache_gradient_buffer(n2w_cache* cache, float** d_grad, int64_t* count, float** d_loss_sum);
+/* One Adam step on grad_scale * (the gradient buffer); clears the buffer. */
+int n2w_cache_apply_gradients(n2w_cache* cache, float grad_scale, n2w_stream_t stream);
 /* Stream-ordered device copy of the parameters (FP32 master and FP16 working
  * copy) of src into dst, which must have the same configuration: the snapshot
  * step of progressive estimation.  Adam state and gradients are not copied. */
@@ -436,6 +443,19 @@ typedef struct n2w_nc_train_options {
  * every step when given). */
 int n2w_nc_train(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* problem,
                  const n2w_nc_train_options* options, float* h_losses, n2w_stream_t stream);
+
+/* Data-parallel online training, one process per GPU: every rank draws its own
+ * fresh points (rank r keyed by seed + r * 0xD6E8FEB86659FD93) and WoS labels,
+ * computes the mean gradient of its batch, the gradients are summed over the
+ * communicator's ranks (NCCL all-reduce) and every rank applies the same Adam
+ * step to the mean of the rank means -- the gradient of the union batch, since
+ * every rank's batch has options->batch points.  Caches start from the same
+ * parameters on every rank (same config and seed) and stay identical.  With a
+ * one-rank communicator this is n2w_nc_train.  h_losses: the union batch's loss
+ * per step (synchronises every step when given).  No counterpart in the
+ * reference (one process, one GPU). */
+int n2w_nc_train_dp(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* problem,
+                    const n2w_nc_train_options* options, n2w_comm* comm, float* h_losses, n2w_stream_t stream);
 
 typedef struct n2w_nc2lmc_options {
   int32_t coarse_walks;     /* walks per point truncated at depth_m, closed by the cache */
@@ -745,6 +765,34 @@ int n2w_count_samples(const uint8_t* d_needs_cache, const int* d_forced, const i
                       unsigned long long* d_counts3, n2w_stream_t stream);
 
 /* ---- thin device-memory helpers for callers without a CUDA binding ------ */
+/* ---- multi-GPU exchange (NCCL, one process per GPU) --------------------- */
+/* Walks and points shard with no communication; ranks exchange only sums of
+ * per-point statistics, timings and (data-parallel training) gradients, as
+ * all-reduces of caller-owned device buffers on the caller's stream.  Rank 0
+ * creates the id with n2w_comm_unique_id and hands its N2W_COMM_ID_BYTES bytes
+ * to every rank (any host channel); each rank then calls n2w_comm_create with
+ * its own device current.  No counterpart in the reference. */
+#define N2W_COMM_ID_BYTES 128
+#define N2W_DTYPE_F32 0
+#define N2W_DTYPE_F64 1
+#define N2W_DTYPE_U32 2
+#define N2W_DTYPE_U64 3
+#define N2W_DTYPE_I32 4
+#define N2W_OP_SUM 0
+#define N2W_OP_MAX 1
+#define N2W_OP_MIN 2
+int n2w_comm_unique_id(uint8_t* id_out);
+int n2w_comm_create(const uint8_t* id, int world, int rank, n2w_comm** out);
+int n2w_comm_info(const n2w_comm* comm, int* rank, int* world);
+int n2w_comm_allreduce(n2w_comm* comm, const void* d_send, void* d_recv, int64_t count, int dtype, int op,
+                       n2w_stream_t stream);
+/* In place: FP64 sum and sum of squares, u32 count, and steps / forced when
+ * non-null, summed over ranks (combines walk shards of the same points). */
+int n2w_comm_allreduce_point_stats(n2w_comm* comm, n2w_point_stats stats, int64_t n, n2w_stream_t stream);
+/* All ranks reach this call before any returns (synchronises `stream`). */
+int n2w_comm_barrier(n2w_comm* comm, n2w_stream_t stream);
+void n2w_comm_destroy(n2w_comm* comm);
+
 int n2w_device_count(int* out);
 int n2w_set_device(int device);
 int n2w_malloc(void** d_ptr, size_t bytes);

@@ -33,7 +33,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{CUDA_HOME / 'include'}"]
 
-LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu", "util.cu", "batch.cu", "server.cu", "probe.cu"]
+LIB_CU = ["closest_point.cu", "walker.cu", "cache.cu", "nc.cu", "util.cu", "batch.cu", "server.cu", "probe.cu", "comm.cu"]
 LIB_CPP = ["mesh.cpp", "bvh_build.cpp", "capi.cpp"]
 EXECUTABLES = {
     "n2wos_probe_cuda_bvh": ["probe_cuda_bvh.cpp"],
@@ -89,7 +89,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         tobjs = {Path(f.result()).name: f.result() for f in tfuts}
     so = LIB / "libn2w.so"
     if _stale(so, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", str(so)] + [str(o) for o in objs] + ["-lcudart"])
+        _run([NVCC] + ARCH + ["-shared", "-o", str(so)] + [str(o) for o in objs] + ["-lcudart", "-lnccl"])
         if verbose:
             print(f"linked {so}")
     for exe, parts in EXECUTABLES.items():

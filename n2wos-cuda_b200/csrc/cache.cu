@@ -925,6 +925,31 @@ int n2w_cache_train_step(n2w_cache* c, const float* d_inputs, const float* d_tar
   });
 }
 
+int n2w_cache_gradient_buffer(n2w_cache* c, float** d_grad, int64_t* count, float** d_loss_sum) {
+  return guarded([&] {
+    N2W_REQUIRE(c, "null cache");
+    if (d_grad) *d_grad = c->d_g;
+    if (count) *count = c->n_total;
+    if (d_loss_sum) *d_loss_sum = c->d_loss;
+  });
+}
+
+int n2w_cache_apply_gradients(n2w_cache* c, float grad_scale, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(c, "null cache");
+    N2W_REQUIRE(std::isfinite(grad_scale) && grad_scale > 0.0f, "grad_scale must be positive");
+    ++c->step;
+    const float b1 = c->cfg.beta1, b2 = c->cfg.beta2;
+    const float bc1 = 1.0f - std::pow(b1, static_cast<float>(c->step));
+    const float bc2 = 1.0f - std::pow(b2, static_cast<float>(c->step));
+    const int b = 256;
+    adam_kernel<<<static_cast<unsigned>((c->n_total + b - 1) / b), b, 0, stream>>>(
+        c->d_p, c->d_ph, c->d_g, c->d_m, c->d_v, c->n_total, c->cfg.learning_rate, b1, b2, c->cfg.epsilon, bc1, bc2,
+        grad_scale);
+    N2W_CUDA(cudaGetLastError());
+  });
+}
+
 int n2w_cache_get_params(const n2w_cache* c, float* h_fp32, uint16_t* h_fp16, float* h_grad) {
   return guarded([&] {
     N2W_REQUIRE(c, "null cache");

@@ -208,6 +208,82 @@ int n2w_nc_train(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* proble
   });
 }
 
+int n2w_nc_train_dp(n2w_cache* cache, const n2w_bvh* bvh, const n2w_problem* problem,
+                    const n2w_nc_train_options* o, n2w_comm* comm, float* h_losses, n2w_stream_t stream) {
+  return guarded([&] {
+    N2W_REQUIRE(cache && bvh && problem && o && comm, "null argument");
+    N2W_REQUIRE(o->steps >= 0 && o->batch > 0 && o->walks_per_label > 0, "invalid training options");
+    auto ok = [](int st) {
+      if (st != N2W_OK) throw Error(st, n2w_last_error());
+    };
+    int rank = 0, world = 1;
+    ok(n2w_comm_info(comm, &rank, &world));
+    float* d_grad = nullptr;
+    float* d_loss = nullptr;
+    int64_t n_params = 0;
+    ok(n2w_cache_gradient_buffer(cache, &d_grad, &n_params, &d_loss));
+    const int64_t B = o->batch;
+    n2w_vec3* pts = stream_alloc<n2w_vec3>(B, stream);
+    float* inputs = stream_alloc<float>(3 * B, stream);
+    float* targets = stream_alloc<float>(B, stream);
+    double* sum = stream_alloc<double>(B, stream);
+    double* sum2 = stream_alloc<double>(B, stream);
+    uint32_t* cnt = stream_alloc<uint32_t>(B, stream);
+    uint64_t* steps = stream_alloc<uint64_t>(B, stream);
+    uint32_t* forced = stream_alloc<uint32_t>(B, stream);
+    unsigned long long* sc = stream_alloc<unsigned long long>(2, stream);
+    void* ws = stream_alloc<char>(n2w_wos_workspace_bytes(B), stream);
+    n2w_point_stats st{sum, sum2, cnt, steps, forced};
+    n2w_walk_options wo{};
+    wo.walks_per_point = o->walks_per_label;
+    wo.max_steps = o->max_steps;
+    wo.epsilon = o->epsilon;
+    wo.step_scale = o->step_scale;
+    // rank r draws its own points and walks; rank 0 draws what n2w_nc_train draws
+    const uint64_t rank_seed = o->seed + 0xD6E8FEB86659FD93ull * static_cast<uint64_t>(rank);
+    int status = N2W_OK;
+    std::string err;
+    for (int s = 0; s < o->steps && status == N2W_OK; ++s) {
+      const uint64_t seed = rank_seed + 0x9E3779B97F4A7C15ull * static_cast<uint64_t>(s + 1);
+      sample_interior(*bvh, o->sample_lo, o->sample_hi, B, seed, pts, sc, stream);
+      wo.seed = seed ^ 0xD1B54A32D192ED03ull;
+      status = n2w_wos_estimate(bvh, problem, pts, B, &wo, st, nullptr, ws, stream);
+      if (status != N2W_OK) {
+        err = n2w_last_error();
+        break;
+      }
+      const int b = 256;
+      labels_kernel<<<static_cast<unsigned>((B + b - 1) / b), b, 0, stream>>>(
+          pts, sum, cnt, B, make_float3(o->input_min[0], o->input_min[1], o->input_min[2]),
+          make_float3(o->input_extent[0], o->input_extent[1], o->input_extent[2]), inputs, targets);
+      N2W_CUDA(cudaGetLastError());
+      // local mean gradient and loss sum -> summed over ranks -> Adam on the mean
+      status = n2w_cache_gradients(cache, inputs, targets, B, nullptr, stream);
+      if (status == N2W_OK && world > 1) {
+        status = n2w_comm_allreduce(comm, d_grad, d_grad, n_params, N2W_DTYPE_F32, N2W_OP_SUM, stream);
+        if (status == N2W_OK) status = n2w_comm_allreduce(comm, d_loss, d_loss, 1, N2W_DTYPE_F32, N2W_OP_SUM, stream);
+      }
+      if (status == N2W_OK) status = n2w_cache_apply_gradients(cache, 1.0f / static_cast<float>(world), stream);
+      if (status != N2W_OK) {
+        err = n2w_last_error();
+        break;
+      }
+      if (h_losses) {
+        float l = 0.0f;
+        N2W_CUDA(cudaMemcpyAsync(&l, d_loss, sizeof(float), cudaMemcpyDeviceToHost, stream));
+        N2W_CUDA(cudaStreamSynchronize(stream));
+        h_losses[s] = l / static_cast<float>(B * world);
+      }
+    }
+    for (void* p : {static_cast<void*>(pts), static_cast<void*>(inputs), static_cast<void*>(targets),
+                    static_cast<void*>(sum), static_cast<void*>(sum2), static_cast<void*>(cnt),
+                    static_cast<void*>(steps), static_cast<void*>(forced), static_cast<void*>(sc), ws}) {
+      scratch_free(p, stream);
+    }
+    if (status != N2W_OK) throw Error(status, err);
+  });
+}
+
 int n2w_nc_progressive(n2w_cache* theta_train, n2w_cache* theta_infer, const n2w_bvh* bvh,
                        const n2w_problem* problem, const n2w_vec3* d_points, int64_t n,
                        const n2w_nc_progressive_options* o, n2w_point_stats coarse, n2w_point_stats residual,

@@ -167,6 +167,8 @@ N2W_REQUEST_PENDING, N2W_REQUEST_ACTIVE, N2W_REQUEST_DONE, N2W_REQUEST_CAPPED, N
 N2W_REQUEST_MODE_PLAIN, N2W_REQUEST_MODE_NC2LMC = 0, 1
 N2W_LABEL_EXACT, N2W_LABEL_WOS = 0, 1
 N2W_SLICE_RULE_RENDER, N2W_SLICE_RULE_EVAL = 0, 1
+N2W_DTYPE_F32, N2W_DTYPE_F64, N2W_DTYPE_U32, N2W_DTYPE_U64, N2W_DTYPE_I32 = range(5)
+N2W_OP_SUM, N2W_OP_MAX, N2W_OP_MIN = range(3)
 
 P = C.c_void_p
 I = C.c_int
@@ -232,6 +234,8 @@ _SIGS = {
     "n2w_cache_gradients": (I, [P, P, P, I64, P, P]),
     "n2w_cache_train_step": (I, [P, P, P, I64, C.POINTER(C.c_float), P]),
     "n2w_cache_zero_grad": (I, [P, P]),
+    "n2w_cache_gradient_buffer": (I, [P, C.POINTER(P), C.POINTER(C.c_int64), C.POINTER(P)]),
+    "n2w_cache_apply_gradients": (I, [P, C.c_float, P]),
     "n2w_cache_copy_params": (I, [P, P, P]),
     "n2w_cache_get_params": (I, [P, P, P, P]),
     "n2w_cache_set_params": (I, [P, P]),
@@ -241,6 +245,7 @@ _SIGS = {
     "n2w_sample_interior_ex": (I, [P, P, P, I64, C.c_uint64, P, C.POINTER(I64), C.POINTER(I64), P]),
     "n2w_map_to_unit": (I, [P, I64, P, P, P, P]),
     "n2w_nc_train": (I, [P, P, C.POINTER(Problem), C.POINTER(NcTrainOptions), P, P]),
+    "n2w_nc_train_dp": (I, [P, P, C.POINTER(Problem), C.POINTER(NcTrainOptions), P, P, P]),
     "n2w_nc_progressive": (I, [P, P, P, C.POINTER(Problem), P, I64, C.POINTER(NcProgressiveOptions), PointStats,
                                PointStats, P, P, P]),
     "n2w_nc2lmc_estimate": (I, [P, C.POINTER(Problem), P, P, I64, C.POINTER(Nc2lmcOptions), PointStats,
@@ -286,6 +291,13 @@ _SIGS = {
     "n2w_stream_create": (I, [PP]),
     "n2w_stream_destroy": (I, [P]),
     "n2w_stream_sync": (I, [P]),
+    "n2w_comm_unique_id": (I, [P]),
+    "n2w_comm_create": (I, [P, I, I, C.POINTER(P)]),
+    "n2w_comm_info": (I, [P, C.POINTER(I), C.POINTER(I)]),
+    "n2w_comm_allreduce": (I, [P, P, P, C.c_int64, I, I, P]),
+    "n2w_comm_allreduce_point_stats": (I, [P, PointStats, C.c_int64, P]),
+    "n2w_comm_barrier": (I, [P, P]),
+    "n2w_comm_destroy": (None, [P]),
     "n2w_device_sync": (I, []),
     "n2w_timer_create": (I, [PP]),
     "n2w_timer_start": (I, [P, P]),

@@ -295,3 +295,41 @@ def test_config1_full_slice_properties(gpu):
     assert 0.9 < za.var() < 1.3, za.var()
     assert 0.90 < np.mean(np.abs(za) < 1.96) < 0.975, np.mean(np.abs(za) < 1.96)
     assert abs(np.corrcoef(za, zc)[0, 1]) < 5.0 / np.sqrt(n), np.corrcoef(za, zc)[0, 1]
+
+
+def config0_points(gpu, bvh, n=4096, radius=0.9, seed=2024):
+    """Points uniform in the ball of radius `radius`, rejected when the mesh's
+    ray-parity test puts them outside, until n are kept."""
+    rng = np.random.default_rng(seed)
+    kept = []
+    while sum(len(k) for k in kept) < n:
+        c = rng.uniform(-radius, radius, (4 * n, 3)).astype(np.float32)
+        c = c[np.einsum("ij,ij->i", c, c) < radius * radius]
+        kept.append(c[bvh.inside(c).astype(bool)])
+    return np.ascontiguousarray(np.concatenate(kept)[:n])
+
+
+def test_config0_wos_at_spec(gpu):
+    """Config 0 at its stated size: the 128 x 256 bumpy sphere r = 1 + 0.08 sin(6t)
+    cos(8p) (65,024 triangles), normalised; seeded 8-charge shell boundary
+    (r in [1.6, 2.0]); 4,096 interior points uniform in r < 0.9; 256 walks,
+    eps = 1e-3, 256-step cap.  The slice MSE against the FP64 solution equals
+    the estimator variance (standardised errors N(0, 1)), nothing is forced."""
+    m = gpu.Mesh.bumpy_sphere_trig(128, 256, 0.08, 6, 8)
+    m.normalize()
+    assert m.counts[1] == 65024
+    bvh = gpu.Bvh(m, 4, "sah")
+    pts = config0_points(gpu, bvh)
+    p = gpu.problem_charges_seeded(8, 1.6, 2.0, 12345)
+    r, cnt = gpu.wos_estimate(bvh, p, pts, options=gpu.walk_options(walks_per_point=256, epsilon=1e-3,
+                                                                     max_steps=256, seed=7))
+    assert cnt["walks"] == 4096 * 256 and cnt["overflow"] == 0 and cnt["forced"] == 0
+    exact = gpu.problem_exact(p, pts.astype(np.float64))
+    err = r["mean"] - exact
+    z = err / r["stderr"]
+    mse = float(np.mean(err ** 2))
+    var = float(np.mean(r["stderr"] ** 2))
+    # the epsilon-shell bias is far below the Monte Carlo error at 256 walks
+    assert abs(float(np.mean(z))) < 4 / np.sqrt(len(z))
+    assert 0.9 < float(np.mean(z ** 2)) < 1.12, (mse, var)
+    assert mse < 1.2 * var

@@ -1,16 +1,43 @@
 """Multi-rank host logic (n2w.shard) with 2-rank gloo groups on CPU: point
 ranges partition the job, walk shares sum to the walk count, rank seeds are
 distinct, and combining walk shards by all-reduce equals one process holding
-every sample; point shards gather back in order."""
+every sample; point shards gather back in order; data-parallel cache training
+(the convention of n2w_nc_train_dp: every rank's mean gradient over its own
+batch, summed over ranks, Adam on the sum / world) equals one process training
+on the union batch, checked with the FP64 cache oracle.
+
+The product's transport is NcclComm (NCCL through the C ABI, one process per
+GPU); these CPU tests drive the same shard functions through GlooComm, a
+test-only communicator over torch.distributed's gloo backend."""
 import os
 import socket
 
 import numpy as np
 import pytest
+import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from n2w import shard
+
+
+class GlooComm:
+    """Test communicator with NcclComm's host interface over gloo."""
+
+    def __init__(self):
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+
+    def allreduce_host(self, arrays, op="sum"):
+        red = {"sum": dist.ReduceOp.SUM, "max": dist.ReduceOp.MAX, "min": dist.ReduceOp.MIN}[op]
+        out = []
+        for a in arrays:
+            t = torch.from_numpy(np.ascontiguousarray(a, np.float64).copy())
+            dist.all_reduce(t, op=red)
+            out.append(t.numpy())
+        return out
+
+    def barrier(self):
+        dist.barrier()
 
 
 def test_point_ranges_partition():
@@ -45,11 +72,12 @@ def _worker(rank, world, port, out_dir):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
+        comm = GlooComm()
         v = samples(rank, world)
-        comb = shard.allreduce_point_stats(stats_of(v))
+        comb = shard.allreduce_point_stats(stats_of(v), comm)
         n = 53
         s, c = shard.point_range(n, rank, world)
-        gathered = shard.gather_point_ranges(np.arange(s, s + c, dtype=np.float64) * 2.0, n)
+        gathered = shard.gather_point_ranges(np.arange(s, s + c, dtype=np.float64) * 2.0, n, comm)
         np.savez(os.path.join(out_dir, f"r{rank}.npz"), mean=comb["mean"], var=comb["sample_variance"],
                  count=comb["count"], gathered=gathered)
     finally:
@@ -73,3 +101,61 @@ def test_two_rank_gloo_combination(tmp_path):
         np.testing.assert_allclose(d["var"], ref["sample_variance"], rtol=1e-9)
         assert np.all(d["count"] == 40)
         np.testing.assert_array_equal(d["gathered"], np.arange(53) * 2.0)
+
+
+# ---- data-parallel training algebra ------------------------------------------------
+
+def dp_problem(seed=5):
+    from oracle import cache_oracle as co
+
+    lay = co.layout(4, 10, 4.0, 32.0, 0.0, 16, 1)
+    rng = np.random.default_rng(seed)
+    params = np.concatenate([rng.uniform(-1e-2, 1e-2, lay["grid_params"]),
+                             rng.uniform(-0.3, 0.3, lay["mlp"]["total"])])
+    B = 64  # per rank
+    u = rng.uniform(0, 1, (2 * B, 3))
+    t = np.sin(3 * u[:, 0]) * np.cos(2 * u[:, 1]) + u[:, 2]
+    return lay, params, u, t, B
+
+
+def adam(p, g, m, v, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-15):
+    """The product's Adam update (FP32 kernel restated in FP64)."""
+    m = b1 * m + (1 - b1) * g
+    v = b2 * v + (1 - b2) * g * g
+    p = p - lr * (m / (1 - b1 ** step)) / (np.sqrt(v / (1 - b2 ** step)) + eps)
+    return p, m, v
+
+
+def _dp_worker(rank, world, port, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import cache_oracle as co
+
+        comm = GlooComm()
+        lay, p, u, t, B = dp_problem()
+        m, v = np.zeros_like(p), np.zeros_like(p)
+        for step in (1, 2, 3):
+            lo = rank * B
+            _, g = co.gradients(lay, p, u[lo:lo + B], t[lo:lo + B])  # mean over this rank's batch
+            g = comm.allreduce_host([g], "sum")[0] / world
+            p, m, v = adam(p, g, m, v, step)
+        np.save(os.path.join(out_dir, f"p{rank}.npy"), p)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_gradients_equal_union_batch(tmp_path):
+    from oracle import cache_oracle as co
+
+    world = 2
+    mp.spawn(_dp_worker, args=(world, free_port(), str(tmp_path)), nprocs=world, join=True)
+    lay, p, u, t, B = dp_problem()
+    m, v = np.zeros_like(p), np.zeros_like(p)
+    for step in (1, 2, 3):
+        _, g = co.gradients(lay, p, u, t)  # one process, the union batch of 2B points
+        p, m, v = adam(p, g, m, v, step)
+    p0, p1 = np.load(tmp_path / "p0.npy"), np.load(tmp_path / "p1.npy")
+    np.testing.assert_array_equal(p0, p1)  # ranks stay identical
+    np.testing.assert_allclose(p0, p, rtol=1e-10, atol=1e-13)
