@@ -299,9 +299,11 @@ int n2w_wos_estimate(const n2w_bvh* bvh, const n2w_problem* problem, const n2w_v
  * path, since cudaMalloc can synchronise the device).  The walker scratch lives
  * in one static device array of N2W_NOALLOC_SCRATCH_BYTES (4 MiB), held by every
  * GPU that loads the library until exit; point_count above N2W_NOALLOC_MAX_POINTS
- * returns N2W_EINVAL.  The caller still passes points and outputs.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress,
- * with that device current): make that first call before any stream capture.
+ * returns N2W_EINVAL.  The caller still passes points and outputs.  Every
+ * call looks up the array's device address (cudaGetSymbolAddress, with the
+ * current device; it allocates nothing, and stays right after a
+ * cudaDeviceReset); the first call on a device also loads the module, so make
+ * that first call before any stream capture.
  * All calls on a device share the one array, so calls that overlap on the GPU
  * (other streams, other threads) race: serialise them.  No cudaMalloc /
  * cudaFree or other allocating routine is called. */

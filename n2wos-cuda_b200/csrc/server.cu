@@ -29,11 +29,13 @@
 //    FP64 additions.
 //  * NC+2LMC requests.  A request in N2W_REQUEST_MODE_NC2LMC uses the cache
 //    registered for its (mesh, problem) with n2w_server_set_nc.  Its sweeps
-//    run between the ticks as fixed chunks of kNcChunk points through
-//    n2w_nc2lmc_estimate_ex on the request's own BVH (coarse walks truncated
-//    at depth m and closed by the cache, plus residual walks), each chunk
-//    keyed by (request seed, sweep, chunk index), so these requests are also
-//    the same alone and in a mix.  The chunk's statistics land in a scratch
+//    run as fixed chunks of kNcChunk points through n2w_nc2lmc_estimate_ex
+//    on the request's own BVH (coarse walks truncated at depth m and closed by
+//    the cache, plus residual walks) on a second stream: each worker
+//    iteration enqueues the plain tick and the NC+2LMC chunks before waiting
+//    for either, so their kernels share the device.  Each chunk is keyed by
+//    (request seed, sweep, chunk index), so these requests are also the same
+//    alone and in a mix.  The chunk's statistics land in a scratch
 //    area and are added to the request's totals; convergence uses the
 //    estimator's standard error sqrt(var_c / N_c + var_r / N_r).
 //
@@ -257,6 +259,8 @@ struct n2w_server {
   n2w_walk_counters* h_counters = nullptr;  // pinned
   char* d_nc_scratch = nullptr;  // one chunk's coarse + residual statistics
   cudaEvent_t ev_tick0 = nullptr, ev_tick1 = nullptr;  // brackets a tick's walker launches
+  cudaStream_t nc_stream = nullptr;  // NC+2LMC chunks, concurrent with the plain tick
+  cudaEvent_t ev_admitted = nullptr;  // admission uploads done (nc_stream waits on it)
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -449,9 +453,15 @@ struct Slice {
   int64_t first, count;  // point range of this tick
 };
 
-// One tick: share the walk budget, launch the batched walker over every
-// active request's next point range, advance cursors, check finished sweeps.
-void tick(n2w_server& s) {
+// One tick, enqueued: share the walk budget and launch the batched walker over
+// every active plain request's next point range on s.stream.  tick_finish
+// synchronises, advances cursors and checks finished sweeps.
+struct TickWork {
+  std::vector<Slice> slices;
+};
+
+TickWork tick_launch(n2w_server& s) {
+  TickWork tw;
   std::vector<n2w_server::Request*> act;
   {
     std::lock_guard<std::mutex> lk(s.mu);
@@ -460,7 +470,7 @@ void tick(n2w_server& s) {
       if (!r->nc) act.push_back(r);
     }
   }
-  if (act.empty()) return;
+  if (act.empty()) return tw;
   // The tick's walk budget goes to the requests with the least remaining
   // sweep work first (shortest remaining work first keeps small requests
   // fast); below, every request still advances by at least one point per tick.
@@ -483,7 +493,7 @@ void tick(n2w_server& s) {
     give[k] = std::min(want[k], left);
     left -= give[k];
   }
-  std::vector<Slice> slices;
+  std::vector<Slice>& slices = tw.slices;
   int64_t tick_points = 0;
   for (size_t k = 0; k < act.size(); ++k) {
     auto* r = act[k];
@@ -495,7 +505,7 @@ void tick(n2w_server& s) {
     slices.push_back({r, r->cursor, pts});
     tick_points += pts;
   }
-  if (slices.empty()) return;
+  if (slices.empty()) return tw;
   const int chunk = s.opt.chunk > 0 ? s.opt.chunk : 1;
   int64_t cbase = 0, pbase = 0;
   for (size_t i = 0; i < slices.size(); ++i) {
@@ -545,16 +555,19 @@ void tick(n2w_server& s) {
   launch_walker_batch(a, s.opt.block_size > 0 ? s.opt.block_size : kDefaultWalkerThreads, 0, 0, st);
   N2W_CUDA(cudaEventRecord(s.ev_tick1, st));
   N2W_CUDA(cudaMemcpyAsync(s.h_counters, s.d_hdr + 256, sizeof(n2w_walk_counters), cudaMemcpyDeviceToHost, st));
-  // Requests whose sweep ends with this tick: reduce their max stderr.
+  return tw;
+}
+
+void tick_finish(n2w_server& s, TickWork& tw) {
+  const std::vector<Slice>& slices = tw.slices;
+  if (slices.empty()) return;
+  const cudaStream_t st = s.stream;
+  // Requests whose sweep ends with this tick: reduce their standard errors.
   std::vector<n2w_server::Request*> swept;
   for (const Slice& sl : slices) {
     if (sl.first + sl.count == sl.r->req.point_count) swept.push_back(sl.r);
   }
-  if (!swept.empty()) {
-    N2W_CUDA(cudaMemsetAsync(s.d_conv, 0, sizeof(unsigned) * swept.size(), st));
-    N2W_CUDA(cudaMemsetAsync(s.d_conv_sum, 0, sizeof(double) * swept.size(), st));
-    launch_sweep_stderr(s, swept);
-  }
+  if (!swept.empty()) launch_sweep_stderr(s, swept);
   N2W_CUDA(cudaStreamSynchronize(st));
   float tick_ms = 0.0f;
   N2W_CUDA(cudaEventElapsedTime(&tick_ms, s.ev_tick0, s.ev_tick1));
@@ -573,11 +586,18 @@ void tick(n2w_server& s) {
   finish_sweeps(s, swept);
 }
 
-// NC+2LMC work between two ticks: chunks of kNcChunk points, shortest
-// remaining sweep first, until tick_walks coarse + residual walks have run
-// (at least one chunk).  Each chunk is keyed by (request seed, sweep, chunk
-// index) alone.
-void nc_step(n2w_server& s) {
+// NC+2LMC work of one worker iteration, enqueued on s.nc_stream so that it
+// runs on the device concurrently with the plain tick: chunks of kNcChunk
+// points, shortest remaining sweep first, until tick_walks coarse + residual
+// walks are enqueued (at least one chunk).  Each chunk is keyed by (request
+// seed, sweep, chunk index) alone.  nc_finish synchronises and checks sweeps.
+struct NcWork {
+  std::vector<n2w_server::Request*> swept;
+  int64_t chunks = 0, walks = 0;
+};
+
+NcWork nc_launch(n2w_server& s) {
+  NcWork nw;
   std::vector<n2w_server::Request*> act;
   {
     std::lock_guard<std::mutex> lk(s.mu);
@@ -586,13 +606,14 @@ void nc_step(n2w_server& s) {
       if (r->nc) act.push_back(r);
     }
   }
-  if (act.empty()) return;
+  if (act.empty()) return nw;
   auto remaining = [](const n2w_server::Request* r) {
     return (r->req.point_count - r->cursor) * static_cast<int64_t>(r->sweep_walks + r->residual_walks);
   };
   std::stable_sort(act.begin(), act.end(),
                    [&](const n2w_server::Request* a, const n2w_server::Request* b) { return remaining(a) < remaining(b); });
-  const cudaStream_t st = s.stream;
+  const cudaStream_t st = s.nc_stream;
+  N2W_CUDA(cudaStreamWaitEvent(st, s.ev_admitted, 0));  // points and accumulators of new requests
   double* c_sum = reinterpret_cast<double*>(s.d_nc_scratch);
   double* c_sum_sq = c_sum + kNcChunk;
   double* r_sum = c_sum_sq + kNcChunk;
@@ -602,7 +623,7 @@ void nc_step(n2w_server& s) {
   uint32_t* c_forced = c_count + kNcChunk;
   uint32_t* r_count = c_forced + kNcChunk;
   int64_t left = s.opt.tick_walks, chunks = 0, walks = 0;
-  std::vector<n2w_server::Request*> swept;
+  std::vector<n2w_server::Request*>& swept = nw.swept;
   for (auto* r : act) {
     if (left <= 0) break;
     while (left > 0 && r->cursor < r->req.point_count) {
@@ -654,14 +675,25 @@ void nc_step(n2w_server& s) {
     }
     if (r->cursor == r->req.point_count) swept.push_back(r);
   }
-  if (!swept.empty()) launch_sweep_stderr(s, swept);
-  N2W_CUDA(cudaStreamSynchronize(st));
+  nw.chunks = chunks;
+  nw.walks = walks;
+  return nw;
+}
+
+void nc_finish(n2w_server& s, NcWork& nw) {
+  if (nw.chunks == 0) return;
+  N2W_CUDA(cudaStreamSynchronize(s.nc_stream));
+  if (!nw.swept.empty()) {
+    // the standard-error reduction shares its buffers with the tick's: on s.stream, after it
+    launch_sweep_stderr(s, nw.swept);
+    N2W_CUDA(cudaStreamSynchronize(s.stream));
+  }
   {
     std::lock_guard<std::mutex> lk(s.mu);
-    s.stats.nc_chunks += chunks;
-    s.stats.nc_walks += walks;
+    s.stats.nc_chunks += nw.chunks;
+    s.stats.nc_walks += nw.walks;
   }
-  finish_sweeps(s, swept);
+  finish_sweeps(s, nw.swept);
 }
 
 void worker_loop(n2w_server* s) {
@@ -674,10 +706,15 @@ void worker_loop(n2w_server* s) {
     }
     try {
       admit(*s);
+      N2W_CUDA(cudaEventRecord(s->ev_admitted, s->stream));
       const int64_t t0 = now_ns();
-      tick(*s);
+      // plain tick and NC+2LMC chunks are both enqueued before either is
+      // waited for, so their kernels overlap on the device
+      TickWork tw = tick_launch(*s);
+      NcWork nw = nc_launch(*s);
+      tick_finish(*s, tw);
       const int64_t t1 = now_ns();
-      nc_step(*s);
+      nc_finish(*s, nw);
       const int64_t t2 = now_ns();
       std::lock_guard<std::mutex> lk(s->mu);
       s->stats.tick_us += (t1 - t0) / 1000;
@@ -707,6 +744,7 @@ void destroy_server(n2w_server* s) {
   s->cv_done.notify_all();
   if (s->worker.joinable()) s->worker.join();
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->nc_stream) cudaStreamSynchronize(s->nc_stream);
   cudaFree(s->d_pool);
   cudaFree(s->d_insts);
   cudaFree(s->d_cpd);
@@ -723,6 +761,8 @@ void destroy_server(n2w_server* s) {
   cudaFreeHost(s->h_conv_sum);
   cudaFreeHost(s->h_counters);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->nc_stream) cudaStreamDestroy(s->nc_stream);
+  if (s->ev_admitted) cudaEventDestroy(s->ev_admitted);
   if (s->scene) {
     n2w_scene_destroy(s->scene.release());
   }
@@ -807,6 +847,8 @@ int n2w_server_create(const n2w_bvh* const* bvhs, int mesh_count, const n2w_prob
     // coarse sum, sum_sq, residual sum, sum_sq, coarse steps (8 B); coarse count, forced, residual count (4 B)
     N2W_CUDA(cudaMalloc(&s->d_nc_scratch, kNcChunk * (5 * 8 + 3 * 4)));
     N2W_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    N2W_CUDA(cudaStreamCreateWithFlags(&s->nc_stream, cudaStreamNonBlocking));
+    N2W_CUDA(cudaEventCreateWithFlags(&s->ev_admitted, cudaEventDisableTiming));
     N2W_CUDA(cudaEventCreate(&s->ev_tick0));
     N2W_CUDA(cudaEventCreate(&s->ev_tick1));
     s->worker = std::thread(worker_loop, s);

@@ -774,27 +774,19 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[N2W_NOALLOC_SCR
 
 namespace {
 
-constexpr int kNoallocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kNoallocMaxDevices] = {};
-
 // In host code the array's name is only a host-side stand-in; its device
-// address is looked up once per device, with that device current, and reused.
+// address is looked up with the current device on every call
+// (cudaGetSymbolAddress allocates nothing), so the address stays right after a
+// cudaDeviceReset has reloaded the module.  The first lookup on a device loads
+// the module, which is why the first call must come before any stream capture.
 void* noalloc_scratch_current_device() {
-  int dev = 0;
-  N2W_CUDA(cudaGetDevice(&dev));
-  N2W_REQUIRE(dev >= 0 && dev < kNoallocMaxDevices, "device index beyond the allocation-free scratch table");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      throw Error(N2W_ECUDA, std::string("cudaGetSymbolAddress for the allocation-free scratch failed: ") +
-                                 cudaGetErrorString(e));
-    }
-    g_noalloc_ptr[dev] = p;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    throw Error(N2W_ECUDA, std::string("cudaGetSymbolAddress for the allocation-free scratch failed: ") +
+                               cudaGetErrorString(e));
   }
-  return g_noalloc_ptr[dev];
+  return p;
 }
 
 }  // namespace

@@ -66,3 +66,28 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(gpu):
                                       stats.struct(), None, None)
     assert st == 1
     assert b"exceed the limit" in lib.n2w_last_error()
+
+
+def test_noalloc_at_its_maximum_size(gpu):
+    """Exactly N2W_NOALLOC_MAX_POINTS points (the scratch's 512 + 24 n bytes
+    fill the 4 MiB array) with a few walks each: the same counts and steps as
+    the allocating entry point."""
+    from n2w._lib import call
+
+    limit = ((4 << 20) - 512) // 24
+    mesh = gpu.Mesh.bumpy_sphere_trig(32, 64, 0.08, 6, 8)
+    mesh.normalize()
+    bvh = gpu.Bvh(mesh, 4, "sah")
+    pts = np.random.default_rng(5).uniform(-0.4, 0.4, (limit, 3)).astype(np.float32)
+    problem = gpu.problem_charges_seeded(8, 1.6, 2.0, 12345)
+    opts = gpu.walk_options(walks_per_point=4, epsilon=1e-3, seed=9)
+    want, _ = gpu.wos_estimate(bvh, problem, pts, options=opts)
+    d_pts = gpu.DeviceBuffer.from_array(pts)
+    stats = gpu.PointStatsBuffers.allocate(limit)
+    call("n2w_wos_estimate_noalloc", bvh.handle, C.byref(problem), d_pts.ptr, limit, C.byref(opts),
+         stats.struct(), None, None)
+    call("n2w_device_sync")
+    got = stats.download()
+    assert np.array_equal(got["count"], want["count"]) and (got["count"] == 4).all()
+    assert np.array_equal(got["mean_steps"], want["mean_steps"])
+    assert np.allclose(got["sum"], want["sum"], rtol=RTOL, atol=1e-12)
