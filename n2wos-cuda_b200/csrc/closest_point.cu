@@ -43,13 +43,21 @@ namespace {
 // dev::traverse, so results and node-visit / triangle-test counts are
 // identical to the one-query-per-thread traversal.
 constexpr int kQueryBlock = 256;
+// Traversal units (node expansions + triangle tests) a lane spends on one
+// query before handing it to the warp-cooperative finisher; the few queries
+// far from the surface in every direction (near the centre of a closed mesh)
+// need thousands, and one of them per lane would set the launch's length.
+constexpr uint32_t kQueryBudget = 320;
+constexpr int kHandOff = 2;         // overflow-slot mark of a handed-off query
+constexpr int kFinishWarps = 4;     // warps per finisher block
+constexpr int kFinishStack = 2048;  // work-list entries per finisher warp (16 KiB)
 
 template <bool kMasked, bool kCount>
 __global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
     const float4* __restrict__ nodes, const float4* __restrict__ tris, const dev::SeedGrid grid,
     const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
     float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
-    int* __restrict__ out_overflow, int* __restrict__ out_nodes, int* __restrict__ out_tris) {
+    int* __restrict__ out_overflow, int* __restrict__ out_nodes, int* __restrict__ out_tris, uint32_t budget) {
   // next unclaimed query of this block's range (unsigned: after the range
   // runs out each lane claims once more, up to b_end + blockDim.x <= 2^31 + 1023)
   __shared__ unsigned s_next;
@@ -108,7 +116,15 @@ __global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
     if (!__any_sync(0xffffffffu, busy)) break;
     if (busy) {
       bool ov = false;
-      if (!dev::trav_step(nodes, tris, p, hit, tv, stack, c_nodes, c_tris, ov)) {
+      if (!kCount && budget && c_nodes + c_tris > budget) {
+        // Over budget: hand the query to the warp-cooperative finisher with its
+        // best so far (a bound on the answer) in its own output slots.
+        out_d2[q] = hit.d2;
+        out_cp[q] = n2w_vec3{hit.cp.x, hit.cp.y, hit.cp.z};
+        out_id[q] = hit.id == INT32_MAX ? -1 : hit.id;
+        out_overflow[q] = kHandOff;
+        busy = false;
+      } else if (!dev::trav_step(nodes, tris, p, hit, tv, stack, c_nodes, c_tris, ov)) {
         out_d2[q] = hit.d2;
         out_cp[q] = n2w_vec3{hit.cp.x, hit.cp.y, hit.cp.z};
         out_id[q] = hit.id == INT32_MAX ? -1 : hit.id;
@@ -121,6 +137,127 @@ __global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
       }
       if (ov) overflow = true;
     }
+  }
+}
+
+// Warp-cooperative finisher for the queries that ran over the per-lane
+// budget (marked kHandOff in their overflow slot): one warp per group of 32
+// consecutive queries takes its marked queries one at a time and traverses
+// the BVH from the root with the lane's best so far as the bound.  A
+// shared-memory work list of (node or leaf, box distance) entries feeds the 32
+// lanes: each iteration every lane takes one entry, expands a node (children
+// whose box is within the warp's best are pushed) or tests a leaf's
+// triangles, and the warp's best (d2, id) -- a 64-bit key, lowest d2 then
+// lowest id -- is the minimum over lanes.  Pruning is conservative, so the
+// answer is the exact one a single-lane traversal gives.  Blocks whose groups
+// hold no marked query exit at once, so the block scheduler balances the work.
+__device__ __forceinline__ unsigned long long hit_key(float d2, int id) {
+  return (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
+}
+
+__global__ void __launch_bounds__(32 * kFinishWarps) closest_point_finish_kernel(
+    const float4* __restrict__ nodes, const float4* __restrict__ tris, const n2w_vec3* __restrict__ points, int n,
+    float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
+    int* __restrict__ out_overflow) {
+  extern __shared__ int2 s_work[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  int2* work = s_work + warp * kFinishStack;
+  const int64_t q0 = (static_cast<int64_t>(blockIdx.x) * kFinishWarps + warp) * 32;
+  if (q0 >= n) return;
+  const int64_t mine = q0 + lane;
+  unsigned pending = __ballot_sync(0xffffffffu, mine < n && out_overflow[mine] == kHandOff);
+  while (pending) {
+    const int q = static_cast<int>(q0) + __ffs(pending) - 1;
+    pending &= pending - 1;
+    const n2w_vec3 pt = points[q];
+    const dev::V3 p = dev::v3(pt.x, pt.y, pt.z);
+    const int id0 = out_id[q];
+    const unsigned long long start_key = hit_key(out_d2[q], id0 < 0 ? INT32_MAX : id0);
+    unsigned long long best_key = start_key;  // warp-uniform
+    unsigned long long my_key = start_key;
+    dev::V3 my_cp = p;
+    bool dropped = false;  // warp-uniform: the work list was full
+    if (lane == 0) work[0] = make_int2(0, __float_as_int(0.0f));
+    int sp = 1;  // warp-uniform
+    __syncwarp();
+    while (sp > 0) {
+      const int take = min(sp, 32);
+      int2 e = make_int2(kEmptyChild, 0);
+      if (lane < take) e = work[sp - take + lane];
+      __syncwarp();
+      sp -= take;
+      const float bound = __uint_as_float(static_cast<unsigned>(best_key >> 32));
+      int2 c0 = make_int2(kEmptyChild, 0), c1 = c0, c2 = c0, c3 = c0;
+      int nc = 0;
+      if (e.x != kEmptyChild && __int_as_float(e.y) <= bound) {
+        if (e.x >= 0) {
+          float4 lox, hix, loy, hiy, loz, hiz;
+          int4 ch;
+          dev::load_node(nodes, e.x, lox, hix, loy, hiy, loz, hiz, ch);
+          float d[4] = {dev::box_d2(p, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x),
+                        dev::box_d2(p, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y),
+                        dev::box_d2(p, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z),
+                        dev::box_d2(p, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w)};
+          const int r[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (r[k] != kEmptyChild && d[k] <= bound) {
+              const int2 ce = make_int2(r[k], __float_as_int(d[k]));
+              if (nc == 0) c0 = ce;
+              else if (nc == 1) c1 = ce;
+              else if (nc == 2) c2 = ce;
+              else c3 = ce;
+              ++nc;
+            }
+          }
+        } else {
+          const int first = leaf_first(e.x), count = leaf_count(e.x);
+          for (int i = 0; i < count; ++i) {
+            dev::ClosestHit h;
+            h.d2 = FLT_MAX;
+            h.id = INT32_MAX;
+            h.slot = 0;
+            h.cp = p;
+            dev::test_slot(tris, first + i, p, h);
+            const unsigned long long k = hit_key(h.d2, h.id);
+            if (k < my_key) {
+              my_key = k;
+              my_cp = h.cp;
+            }
+          }
+        }
+      }
+      unsigned long long wk = my_key;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) wk = min(wk, __shfl_xor_sync(0xffffffffu, wk, o));
+      best_key = min(best_key, wk);
+      // append this iteration's children (lane order, each lane's nearest last)
+      int incl = nc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      int at = sp + incl - nc;
+      const int2 cs[4] = {c0, c1, c2, c3};
+      for (int j = nc - 1; j >= 0; --j, ++at) {
+        if (at < kFinishStack) work[at] = cs[j];
+      }
+      if (sp + total > kFinishStack) dropped = true;
+      sp = min(sp + total, kFinishStack);
+      __syncwarp();
+    }
+    // the lane holding the winning key writes it (a triangle is tested by one
+    // lane only); if nothing beat the hand-off bound, the written hit stands
+    if (best_key != start_key && my_key == best_key) {
+      out_d2[q] = __uint_as_float(static_cast<unsigned>(best_key >> 32));
+      out_id[q] = static_cast<int>(best_key & 0xffffffffu);
+      out_cp[q] = n2w_vec3{my_cp.x, my_cp.y, my_cp.z};
+    }
+    if (lane == 0) out_overflow[q] = dropped ? 1 : 0;
+    __syncwarp();
   }
 }
 
@@ -192,11 +329,32 @@ void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const ui
     const int64_t blocks_needed = (static_cast<int64_t>(n) + kQueryBlock - 1) / kQueryBlock;
     const int64_t resident = static_cast<int64_t>(sm_count_current()) * std::max(occ, 1);
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min(blocks_needed, resident)));
-    kern<<<grid, kQueryBlock, 0, stream>>>(nodes, tris, sg, d_points, act, n, d_d2, d_cp, d_id, d_overflow, dn, dt);
+    kern<<<grid, kQueryBlock, 0, stream>>>(nodes, tris, sg, d_points, act, n, d_d2, d_cp, d_id, d_overflow, dn, dt,
+                                           dn ? 0u : kQueryBudget);
   };
-  if (d_nodes) launch(closest_point_kernel<false, true>, d_active, d_nodes, d_tris);
-  else if (d_active) launch(closest_point_kernel<true, false>, d_active, nullptr, nullptr);
+  if (d_nodes) {
+    // the counting variant runs every query to completion in one lane, so its
+    // counts are the single-lane traversal's (the algorithmic work)
+    launch(closest_point_kernel<false, true>, d_active, d_nodes, d_tris);
+    N2W_CUDA(cudaGetLastError());
+    return;
+  }
+  if (d_active) launch(closest_point_kernel<true, false>, d_active, nullptr, nullptr);
   else launch(closest_point_kernel<false, false>, nullptr, nullptr, nullptr);
+  N2W_CUDA(cudaGetLastError());
+  const size_t smem = sizeof(int2) * kFinishWarps * kFinishStack;
+  static thread_local int configured_device = -1;
+  int dev = 0;
+  N2W_CUDA(cudaGetDevice(&dev));
+  if (configured_device != dev) {
+    N2W_CUDA(cudaFuncSetAttribute(closest_point_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    configured_device = dev;
+  }
+  const int64_t groups = (static_cast<int64_t>(n) + 31) / 32;
+  const unsigned blocks = static_cast<unsigned>((groups + kFinishWarps - 1) / kFinishWarps);
+  closest_point_finish_kernel<<<blocks, 32 * kFinishWarps, smem, stream>>>(nodes, tris, d_points, n, d_d2, d_cp,
+                                                                          d_id, d_overflow);
   N2W_CUDA(cudaGetLastError());
 }
 

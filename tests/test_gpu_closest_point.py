@@ -46,6 +46,10 @@ def test_config0_queries_vs_oracle(gpu, method, leaf):
     assert_bitexact(r, tr)
     assert np.array_equal(r["node_visits"], tr["node_visits"])
     assert np.array_equal(r["tri_tests"], tr["tri_tests"])
+    # the uncounted launch (long queries finished by whole warps) gives the same answers
+    plain = bvh.query(pts)
+    assert_bitexact(plain, r)
+    assert (plain["overflow"] == 0).all()
     bf = oracle.bruteforce(v, t, pts[:2048])
     sub = {k: r[k][:2048] for k in ("distance2", "closest", "triangle_id")}
     assert_bitexact(sub, bf)
@@ -143,3 +147,36 @@ def test_reference_gpu_kernel_agrees(gpu, bumpy_ref_mesh, golden_closest):
         assert np.max(np.abs(np.sqrt(d2) - np.sqrt(golden_closest["distance2"]))) <= 2e-4
     finally:
         R.ref_gpu_bvh_destroy(C.c_void_p(h))
+
+
+@pytest.mark.parametrize("masked", [False, True])
+def test_long_queries_handed_to_warp_finisher_stay_exact(gpu, masked):
+    """Points near the centre of a closed mesh are far from the surface in every
+    direction, so their traversals run past the per-lane budget and are
+    finished by a whole warp from the lane's best so far.  The answers stay
+    the brute force's bit for bit (lowest id on ties), no overflow slot is left
+    marked, and queries on the surface or far outside (short traversals) in
+    the same launch are unaffected."""
+    m = gpu.Mesh.bumpy_sphere_trig(128, 256, 0.08, 6, 8)
+    m.normalize()
+    bvh = gpu.Bvh(m, 4, "sah")
+    v, t = m.arrays()
+    rng = np.random.default_rng(77)
+    centre = rng.uniform(-0.25, 0.25, (3000, 3)).astype(np.float32)
+    others = rng.uniform(-1.2, 1.2, (3000, 3)).astype(np.float32)
+    pts = np.concatenate([centre, others, v[:200]]).astype(np.float32)
+    active = None
+    if masked:
+        active = (rng.random(len(pts)) < 0.8).astype(np.uint8)
+    got = bvh.query(pts, active=active)
+    want = oracle.bruteforce(v, t, pts)
+    sel = np.ones(len(pts), bool) if active is None else active.astype(bool)
+    assert np.array_equal(got["distance2"][sel].view(np.uint32), want["distance2"][sel].view(np.uint32))
+    assert np.array_equal(got["triangle_id"][sel], want["triangle_id"][sel])
+    assert np.array_equal(got["closest"][sel].view(np.uint32), want["closest"][sel].view(np.uint32))
+    assert (got["overflow"] == 0).all()
+    if active is not None:
+        assert (got["triangle_id"][~sel] == -1).all() and (got["distance2"][~sel] == 0).all()
+    # the centre queries really are the long ones: their single-lane work exceeds the budget
+    counted = bvh.query(centre[:256], counted=True)
+    assert np.median(counted["node_visits"] + counted["tri_tests"]) > 320
