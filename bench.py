@@ -443,12 +443,12 @@ def measured_time_to_mse(n2w, call, bvh, mesh, pts, exact, problem, cache, best,
     t = n2w.Timer()
     res = {"points": n, "stride": stride, "target_mse": target, "cap_seconds_subsample": cap_s}
 
-    # plain WoS, 16 source samples, blocks of 512 walks per point accumulated on the device
+    # plain WoS, 16 source samples, blocks of 1,024 walks per point accumulated on the device
     st = n2w.PointStatsBuffers.allocate(n)
     ws = n2w.DeviceBuffer(n2w._lib.lib.n2w_wos_workspace_bytes(n))
     total_ms, blocks, mse = 0.0, 0, None
     while total_ms / 1e3 < cap_s:
-        o = n2w.walk_options(walks_per_point=512, epsilon=5e-4, seed=1000 + blocks, accumulate=1 if blocks else 0)
+        o = n2w.walk_options(walks_per_point=1024, epsilon=5e-4, seed=1000 + blocks, accumulate=1 if blocks else 0)
         t.start()
         call("n2w_wos_estimate", bvh.handle, C.byref(problem), dp.ptr, n, C.byref(o), st.struct(), None, ws.ptr, None)
         t.stop()
@@ -459,13 +459,13 @@ def measured_time_to_mse(n2w, call, bvh, mesh, pts, exact, problem, cache, best,
         if mse < target:
             break
     res["plain_16"] = {"reached": bool(mse is not None and mse < target), "mse": mse, "blocks": blocks,
-                       "walks_per_point": 512 * blocks, "seconds_subsample": total_ms / 1e3,
+                       "walks_per_point": 1024 * blocks, "seconds_subsample": total_ms / 1e3,
                        "seconds_full_slice": total_ms / 1e3 * stride}
 
     # NC+2LMC at the trained cache's best depth with its optimal residual fraction
     m = best["depth_m"]
     frac = min(1.0, max(best["optimal_residual_fraction"], 1.0 / 64))
-    wc = 256
+    wc = 1024
     wr = max(1, int(round(wc * frac)))
     acc = {k: [np.zeros(n), np.zeros(n), np.zeros(n)] for k in ("c", "r")}
     total_ms, blocks, mse = 0.0, 0, None

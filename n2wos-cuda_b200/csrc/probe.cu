@@ -21,6 +21,19 @@ constexpr int kProbeThreads = 256;
 constexpr int kProbeBlocksPerSm = 8;
 constexpr size_t kL1Slice4 = 1024;  // float4 per block slice: 16 KiB
 
+// Loads the compiler may not hoist out of the repeat loop or merge across
+// iterations (volatile): L1-caching (.ca) and L2-only (.cg) 16-byte reads.
+__device__ __forceinline__ float4 load_ca(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.ca.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float4 load_cg(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.cg.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+
 __device__ __forceinline__ void acc4(float4& a, float4 v) {
   a.x += v.x;
   a.y += v.y;
@@ -38,14 +51,14 @@ __global__ void __launch_bounds__(kProbeThreads) read_l2_kernel(const float4* __
   for (int it = 0; it < iters; ++it) {
     size_t i = start;
     for (; i + 3 * stride < n4; i += 4 * stride) {
-      const float4 v0 = __ldcg(buf + i), v1 = __ldcg(buf + i + stride), v2 = __ldcg(buf + i + 2 * stride),
-                   v3 = __ldcg(buf + i + 3 * stride);
+      const float4 v0 = load_cg(buf + i), v1 = load_cg(buf + i + stride), v2 = load_cg(buf + i + 2 * stride),
+                   v3 = load_cg(buf + i + 3 * stride);
       acc4(a0, v0);
       acc4(a1, v1);
       acc4(a2, v2);
       acc4(a3, v3);
     }
-    for (; i < n4; i += stride) acc4(a0, __ldcg(buf + i));
+    for (; i < n4; i += stride) acc4(a0, load_cg(buf + i));
   }
   const float s = a0.x + a1.y + a2.z + a3.w + a0.w + a1.x + a2.y + a3.z;
   if (s != 0.0f) sink[start] = make_float4(s, s, s, s);
@@ -58,10 +71,10 @@ __global__ void __launch_bounds__(kProbeThreads) read_l1_kernel(const float4* __
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
     for (size_t j = threadIdx.x; j < kL1Slice4; j += 4 * kProbeThreads) {
-      acc4(a0, __ldca(slice + j));
-      acc4(a1, __ldca(slice + j + kProbeThreads));
-      acc4(a2, __ldca(slice + j + 2 * kProbeThreads));
-      acc4(a3, __ldca(slice + j + 3 * kProbeThreads));
+      acc4(a0, load_ca(slice + j));
+      acc4(a1, load_ca(slice + j + kProbeThreads));
+      acc4(a2, load_ca(slice + j + 2 * kProbeThreads));
+      acc4(a3, load_ca(slice + j + 3 * kProbeThreads));
     }
   }
   const float s = a0.x + a1.y + a2.z + a3.w + a0.w + a1.x + a2.y + a3.z;

@@ -420,6 +420,11 @@ class PointStatsBuffers:
     def struct(self) -> PointStats:
         return PointStats(self.sum.ptr, self.sum_sq.ptr, self.count.ptr, self.steps.ptr, self.forced.ptr)
 
+    def zero(self, stream=None):
+        """Clears every accumulator (device allocations start uninitialised)."""
+        for b in (self.sum, self.sum_sq, self.count, self.steps, self.forced):
+            b.zero(stream)
+
     def download(self, stream=None) -> dict:
         s = self.sum.download(np.float64, self.n, stream)
         s2 = self.sum_sq.download(np.float64, self.n, stream)

@@ -136,8 +136,9 @@ def test_prefix_samples_match_oracle(gpu, scene, name, depth_m):
         o = oracle_samples(nodes, tris, p, pts, seed, oracle.MODE_PREFIX, depth_m)
         for src, (im, iv) in ((g, (0, 1)), (o, (2, 3))):
             needs = src["needs_cache"].astype(bool)
-            # walks that need the cache stopped exactly at depth m
-            assert (src["steps"][needs] == depth_m).all() and (src["steps"][~needs] < depth_m).all()
+            # walks that need the cache stopped exactly at depth m; the others
+            # reached the epsilon shell at or before it (the shell test comes first)
+            assert (src["steps"][needs] == depth_m).all() and (src["steps"][~needs] <= depth_m).all()
             assert ((src["inputs"] >= 0) & (src["inputs"] <= 1)).all()
             for key, arr in (("A", src["value"]), ("needs", needs.astype(np.float64)), ("x", src["inputs"][:, 0]),
                              ("y", src["inputs"][:, 1]), ("z", src["inputs"][:, 2])):
@@ -216,6 +217,7 @@ def test_label_update_matches_oracle(gpu, scene):
     gt, ot, gvar = [], [], []
     for seed in SEEDS:
         acc = gpu.PointStatsBuffers.allocate(n)
+        acc.zero()  # the running accumulators start at zero before refresh 0
         d_in, d_tg = gpu.DeviceBuffer(12 * n), gpu.DeviceBuffer(4 * n)
         otg, ocnt = np.zeros(n, np.float32), np.zeros(n, np.int32)
         for refresh in range(2):

@@ -326,9 +326,13 @@ def test_config0_wos_at_spec(gpu):
     assert cnt["walks"] == 4096 * 256 and cnt["overflow"] == 0 and cnt["forced"] == 0
     exact = gpu.problem_exact(p, pts.astype(np.float64))
     err = r["mean"] - exact
-    z = err / r["stderr"]
     mse = float(np.mean(err ** 2))
     var = float(np.mean(r["stderr"] ** 2))
+    # points already inside the epsilon shell: every walk stops at once at the
+    # same closest point, so there is no variance and the error is O(eps)
+    shell = r["stderr"] == 0
+    assert shell.sum() < 0.01 * len(pts) and np.all(np.abs(err[shell]) < 0.05)
+    z = err[~shell] / r["stderr"][~shell]
     # the epsilon-shell bias is far below the Monte Carlo error at 256 walks
     assert abs(float(np.mean(z))) < 4 / np.sqrt(len(z))
     assert 0.9 < float(np.mean(z ** 2)) < 1.12, (mse, var)
