@@ -362,7 +362,10 @@ def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub
             ms = t.ms()
         r = st.download()
         tw, var = ms / 1e3 / (n * W), float(np.mean(r["sample_variance"]))
-        return {"s_per_walk": tw, "var_per_walk": var, "seconds_extrapolated": nc.time_to_mse(target, P * tw, var, 0.0)}
+        # per-point (Neyman) allocation of walks: N_i proportional to sqrt(V_i)
+        neyman = P * tw * float(np.mean(np.sqrt(r["sample_variance"]))) ** 2 / target
+        return {"s_per_walk": tw, "var_per_walk": var, "seconds_extrapolated": nc.time_to_mse(target, P * tw, var, 0.0),
+                "seconds_per_point_allocation": neyman}
 
     out["plain_wos"] = plain(problem)
     p16 = n2w.problem_sinprod(3.0 * np.pi, n2w.N2W_SOURCE_BALL)
@@ -396,9 +399,13 @@ def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub
             vr = float(np.mean(rr["residual"]["sample_variance"]))
             fixed = train_s if c is not None else 0.0
             opt = fixed + P * (np.sqrt(vc * tc) + np.sqrt(vr * tr)) ** 2 / target
+            # per-point allocation of both levels' walks (sqrt(V_c,i t_c) + sqrt(V_r,i t_r) per point)
+            opt_pp = fixed + P * float(np.mean(np.sqrt(rc["coarse"]["sample_variance"] * tc) +
+                                               np.sqrt(rr["residual"]["sample_variance"] * tr))) ** 2 / target
             levels[f"{cache_kind}_m{m}"] = {
                 "cache": cache_kind, "depth_m": m, "s_per_coarse_walk": tc, "s_per_residual_walk": tr,
                 "var_coarse": vc, "var_residual": vr, "seconds_optimal_allocation": opt,
+                "seconds_per_point_allocation": opt_pp,
                 "seconds_residual_1_16": nc.time_to_mse(target, P * (tc + tr / 16), vc + 16 * vr, 0.0, fixed),
                 "optimal_residual_fraction": float(np.sqrt((vr / tr) / (vc / tc))),
                 "explained_variance_R2": max(0.0, 1.0 - vr / var16),
@@ -416,6 +423,10 @@ def time_to_mse(n2w, lib, call, mesh, bvh, pts, exact, problem, target=1e-4, sub
         best["seconds_optimal_allocation"],
         "best_trained_depth": best["depth_m"],
         "bound_exact_solution_cache_speedup": best_bound["speedup_vs_plain_16_same_walks"],
+        "per_point_allocation_both": out["plain_wos_16_source_samples"]["seconds_per_point_allocation"] /
+        min(v["seconds_per_point_allocation"] for v in trained.values()),
+        "per_point_allocation_bound_exact_cache": out["plain_wos_16_source_samples"]["seconds_per_point_allocation"] /
+        min(v["seconds_per_point_allocation"] for v in bound.values()),
         "bound_depth": best_bound["depth_m"],
         "config2_m8_residual_1_16_speedup_vs_plain_16": out["plain_wos_16_source_samples"]["seconds_extrapolated"] /
         levels["trained_m8"]["seconds_residual_1_16"],
@@ -832,7 +843,7 @@ def run_serve(args):
         sweep.append({"offered_req_per_s": rate, "requests": a.serve_requests, "complete": line["complete"],
                       "finished": line["finished_requests"], "latency_s": line["latency_s"],
                       "throughput": line["throughput"], "accuracy": line["accuracy"],
-                      "nc2lmc": line["modes"]["nc2lmc"], "clocks": line["clocks"]})
+                      "nc2lmc": line["modes"]["nc2lmc"], "server": line["server"], "clocks": line["clocks"]})
         print(f"[serve sweep] rate {rate}: p50 {line['latency_s']['p50']:.3f}s p99<=4096 "
               f"{line['latency_s']['p99_le4096']:.3f}s done {line['finished_requests']}/{a.serve_requests}",
               file=sys.stderr, flush=True)
@@ -1007,7 +1018,10 @@ def serve_line(args):
                       "p50_le4096": float(np.percentile(small, 50)), "p99_le4096": float(np.percentile(small, 99)),
                       "max": float(np.max(lat))},
         "throughput": {"requests_per_s": done / makespan, "points_per_s": sum(r["n"] for r in results) / makespan,
-                       "walk_steps_per_s": st["walk_steps"] / makespan, "makespan_s": makespan},
+                       "walk_steps_per_s": st["walk_steps"] / makespan,
+                       "walks_per_s_incl_nc2lmc": (st["walks"] + st["nc_walks"]) / makespan,
+                       "makespan_s": makespan, "note": "walk_steps_per_s counts the plain ticks' walks; "
+                       "walks_per_s_incl_nc2lmc adds the NC+2LMC chunks' coarse and residual walks"},
         "accuracy": {"median_mse_over_target2": float(np.median(mse_ratio)),
                      "p99_mse_over_target2": float(np.percentile(mse_ratio, 99)),
                      "done": int(sum(r["state"] == 2 for r in results)),

@@ -68,14 +68,16 @@ __global__ void __launch_bounds__(kProbeThreads) read_l1_kernel(const float4* __
                                                                 float4* __restrict__ sink) {
   const float4* slice = buf + static_cast<size_t>(blockIdx.x) * kL1Slice4;
   float4 a0 = make_float4(0, 0, 0, 0), a1 = a0, a2 = a0, a3 = a0;
+  constexpr unsigned kMask = static_cast<unsigned>(kL1Slice4) - 1u;
   for (int it = 0; it < iters; ++it) {
-#pragma unroll
-    for (size_t j = threadIdx.x; j < kL1Slice4; j += 4 * kProbeThreads) {
-      acc4(a0, load_ca(slice + j));
-      acc4(a1, load_ca(slice + j + kProbeThreads));
-      acc4(a2, load_ca(slice + j + 2 * kProbeThreads));
-      acc4(a3, load_ca(slice + j + 3 * kProbeThreads));
-    }
+    // the lane's offsets rotate every pass (a pass still reads the whole
+    // slice, a coalesced 512 B per warp load), so no load repeats the
+    // previous pass's address and none can be hoisted out of the loop
+    const unsigned j = (threadIdx.x + static_cast<unsigned>(it) * 32u) & kMask;
+    acc4(a0, load_ca(slice + j));
+    acc4(a1, load_ca(slice + ((j + kProbeThreads) & kMask)));
+    acc4(a2, load_ca(slice + ((j + 2 * kProbeThreads) & kMask)));
+    acc4(a3, load_ca(slice + ((j + 3 * kProbeThreads) & kMask)));
   }
   const float s = a0.x + a1.y + a2.z + a3.w + a0.w + a1.x + a2.y + a3.z;
   if (s != 0.0f) sink[static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x] = make_float4(s, s, s, s);

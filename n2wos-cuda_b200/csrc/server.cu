@@ -448,6 +448,9 @@ void finish_sweeps(n2w_server& s, const std::vector<n2w_server::Request*>& swept
   }
 }
 
+// In-flight plain requests a tick of tick_walks serves before it grows.
+constexpr int64_t kRequestsPerBaseTick = 8;
+
 struct Slice {
   n2w_server::Request* r;
   int64_t first, count;  // point range of this tick
@@ -484,9 +487,19 @@ TickWork tick_launch(n2w_server& s) {
   }
   // Larger ticks when only large sweeps are in flight: a tick waits for its
   // slowest walk, so more walks per tick fill the GPU better, and no small
-  // request is there to be delayed by the longer tick.
-  const int64_t budget = (!small_in_flight && s.opt.tick_walks_max > s.opt.tick_walks) ? s.opt.tick_walks_max
-                                                                                          : s.opt.tick_walks;
+  // request is there to be delayed by the longer tick.  When many requests
+  // are in flight the queue is building up, and the tick grows with their
+  // number (every request still advances in every tick), trading a longer
+  // tick for the throughput that drains the queue.
+  int64_t budget = s.opt.tick_walks;
+  if (s.opt.tick_walks_max > s.opt.tick_walks) {
+    if (!small_in_flight) {
+      budget = s.opt.tick_walks_max;
+    } else {
+      const int64_t scaled = s.opt.tick_walks * static_cast<int64_t>(act.size()) / kRequestsPerBaseTick;
+      budget = std::min(std::max(scaled, s.opt.tick_walks), s.opt.tick_walks_max);
+    }
+  }
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return want[a] < want[b]; });
   int64_t left = budget;
   for (size_t k : order) {
