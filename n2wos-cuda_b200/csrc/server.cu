@@ -29,12 +29,12 @@
 //    FP64 additions.
 //  * NC+2LMC requests.  A request in N2W_REQUEST_MODE_NC2LMC uses the cache
 //    registered for its (mesh, problem) with n2w_server_set_nc.  Its sweeps
-//    run as fixed chunks of kNcChunk points through n2w_nc2lmc_estimate_ex
+//    run as chunks of up to kNcChunk points (about one tick's walks) through n2w_nc2lmc_estimate_ex
 //    on the request's own BVH (coarse walks truncated at depth m and closed by
 //    the cache, plus residual walks) on a second stream: each worker
 //    iteration enqueues the plain tick and the NC+2LMC chunks before waiting
 //    for either, so their kernels share the device.  Each chunk is keyed by
-//    (request seed, sweep, chunk index), so these requests are also the same
+//    (request seed, sweep, first point of the chunk), so these requests are also the same
 //    alone and in a mix.  The chunk's statistics land in a scratch
 //    area and are added to the request's totals; convergence uses the
 //    estimator's standard error sqrt(var_c / N_c + var_r / N_r).
@@ -165,7 +165,8 @@ size_t request_bytes(int64_t n, bool nc) {
 // Points per NC+2LMC chunk (the unit of work and of walk keying).  Small
 // enough that one chunk (1,024 points x a few thousand walks) stays within
 // a few tens of milliseconds, so NC work interleaves with the plain ticks.
-constexpr int64_t kNcChunk = 1024;
+constexpr int64_t kNcChunk = 1024;   // most points in one NC+2LMC chunk
+constexpr int64_t kNcMinChunk = 32;  // fewest (a chunk may then exceed a tick's walks)
 
 uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -600,10 +601,10 @@ void tick_finish(n2w_server& s, TickWork& tw) {
 }
 
 // NC+2LMC work of one worker iteration, enqueued on s.nc_stream so that it
-// runs on the device concurrently with the plain tick: chunks of kNcChunk
+// runs on the device concurrently with the plain tick: chunks of up to kNcChunk
 // points, shortest remaining sweep first, until tick_walks coarse + residual
 // walks are enqueued (at least one chunk).  Each chunk is keyed by (request
-// seed, sweep, chunk index) alone.  nc_finish synchronises and checks sweeps.
+// seed, sweep, first point of the chunk) alone.  nc_finish synchronises and checks sweeps.
 struct NcWork {
   std::vector<n2w_server::Request*> swept;
   int64_t chunks = 0, walks = 0;
@@ -641,7 +642,14 @@ NcWork nc_launch(n2w_server& s) {
     if (left <= 0) break;
     while (left > 0 && r->cursor < r->req.point_count) {
       const int64_t first = r->cursor;
-      const int64_t np = std::min(kNcChunk, r->req.point_count - first);
+      // Chunk size from the request's own sweep: at most kNcChunk points and at
+      // most about one tick's walks, so a chunk never holds the worker (and the
+      // plain ticks behind it) for much longer than a tick.  It depends on
+      // nothing else in flight, so the chunking -- and the walks -- are the same
+      // alone and in any mix.
+      const int64_t per_point = std::max<int64_t>(1, r->sweep_walks + r->residual_walks);
+      const int64_t span = std::min(kNcChunk, std::max(kNcMinChunk, s.opt.tick_walks / per_point));
+      const int64_t np = std::min(span, r->req.point_count - first);
       n2w_nc2lmc_options o{};
       o.coarse_walks = r->sweep_walks;
       o.residual_walks = r->residual_walks;
@@ -650,7 +658,7 @@ NcWork nc_launch(n2w_server& s) {
       o.epsilon = s.opt.epsilon;
       o.step_scale = s.opt.step_scale;
       o.seed = splitmix64(r->req.seed ^ splitmix64((static_cast<uint64_t>(r->sweep) << 40) +
-                                                   static_cast<uint64_t>(first / kNcChunk)));
+                                                   static_cast<uint64_t>(first)));
       for (int k = 0; k < 3; ++k) {
         o.input_min[k] = r->ncfg.input_min[k];
         o.input_extent[k] = r->ncfg.input_extent[k];
