@@ -33,7 +33,8 @@
 //    on the request's own BVH (coarse walks truncated at depth m and closed by
 //    the cache, plus residual walks) on a second stream: each worker
 //    iteration enqueues the plain tick and the NC+2LMC chunks before waiting
-//    for either, so their kernels share the device.  Each chunk is keyed by
+//    for either, so their kernels share the device; the NC+2LMC walks per
+//    iteration adapt so that the chunks end about when the tick does.  Each chunk is keyed by
 //    (request seed, sweep, first point of the chunk), so these requests are also the same
 //    alone and in a mix.  The chunk's statistics land in a scratch
 //    area and are added to the request's totals; convergence uses the
@@ -262,6 +263,9 @@ struct n2w_server {
   cudaEvent_t ev_tick0 = nullptr, ev_tick1 = nullptr;  // brackets a tick's walker launches
   cudaStream_t nc_stream = nullptr;  // NC+2LMC chunks, concurrent with the plain tick
   cudaEvent_t ev_admitted = nullptr;  // admission uploads done (nc_stream waits on it)
+  // NC+2LMC walks a worker iteration enqueues while plain requests are in
+  // flight; adapted so the chunks end about when the plain tick does
+  int64_t nc_budget = 0;
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -602,9 +606,10 @@ void tick_finish(n2w_server& s, TickWork& tw) {
 
 // NC+2LMC work of one worker iteration, enqueued on s.nc_stream so that it
 // runs on the device concurrently with the plain tick: chunks of up to kNcChunk
-// points, shortest remaining sweep first, until tick_walks coarse + residual
+// points, shortest remaining sweep first, until s.nc_budget coarse + residual
 // walks are enqueued (at least one chunk).  Each chunk is keyed by (request
-// seed, sweep, first point of the chunk) alone.  nc_finish synchronises and checks sweeps.
+// seed, sweep, first point of the chunk) alone, so the number of chunks per
+// iteration changes no estimate.  nc_finish synchronises and checks sweeps.
 struct NcWork {
   std::vector<n2w_server::Request*> swept;
   int64_t chunks = 0, walks = 0;
@@ -636,7 +641,7 @@ NcWork nc_launch(n2w_server& s) {
   uint32_t* c_count = reinterpret_cast<uint32_t*>(c_steps + kNcChunk);
   uint32_t* c_forced = c_count + kNcChunk;
   uint32_t* r_count = c_forced + kNcChunk;
-  int64_t left = s.opt.tick_walks, chunks = 0, walks = 0;
+  int64_t left = s.nc_budget > 0 ? s.nc_budget : s.opt.tick_walks, chunks = 0, walks = 0;
   std::vector<n2w_server::Request*>& swept = nw.swept;
   for (auto* r : act) {
     if (left <= 0) break;
@@ -717,6 +722,23 @@ void nc_finish(n2w_server& s, NcWork& nw) {
   finish_sweeps(s, nw.swept);
 }
 
+// NC+2LMC walk budget of a worker iteration while plain requests are in
+// flight.  A NC+2LMC walk costs several plain walks (residual walks carry the
+// Poisson source samples, coarse walks the cache), so a budget equal to the
+// plain tick's held the worker -- and every plain request -- for up to twice
+// the tick.  Multiplicative steps keep the time the worker waits for the
+// chunks after the tick has ended between 1/16 and 1/4 of the tick.
+constexpr int64_t kNcBudgetMinDivisor = 8;  // floor: tick_walks / 8 (and always one chunk)
+
+void adapt_nc_budget(n2w_server& s, int64_t tick_ns, int64_t wait_ns) {
+  const int64_t hi = std::max(s.opt.tick_walks, s.opt.tick_walks_max);
+  const int64_t lo = std::max<int64_t>(1, s.opt.tick_walks / kNcBudgetMinDivisor);
+  int64_t b = s.nc_budget > 0 ? s.nc_budget : s.opt.tick_walks;
+  if (4 * wait_ns > tick_ns) b = b * 3 / 4;
+  else if (16 * wait_ns < tick_ns) b = b * 5 / 4 + 1;
+  s.nc_budget = std::min(hi, std::max(lo, b));
+}
+
 void worker_loop(n2w_server* s) {
   cudaSetDevice(s->device);
   for (;;) {
@@ -733,10 +755,12 @@ void worker_loop(n2w_server* s) {
       // waited for, so their kernels overlap on the device
       TickWork tw = tick_launch(*s);
       NcWork nw = nc_launch(*s);
+      const bool plain = !tw.slices.empty();
       tick_finish(*s, tw);
       const int64_t t1 = now_ns();
       nc_finish(*s, nw);
       const int64_t t2 = now_ns();
+      if (plain && nw.chunks > 0) adapt_nc_budget(*s, t1 - t0, t2 - t1);
       std::lock_guard<std::mutex> lk(s->mu);
       s->stats.tick_us += (t1 - t0) / 1000;
       s->stats.nc_us += (t2 - t1) / 1000;

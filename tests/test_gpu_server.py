@@ -121,12 +121,12 @@ def test_nc2lmc_requests_alone_equal_mix_and_unbiased(gpu, meshes):
     srv.set_nc(1, 1, None, *nc.input_box(m1), depth_m=2, residual_fraction=0.5)
     with pytest.raises(gpu.N2wError, match="no cache registered"):
         srv.submit(1, 0, points(meshes, 1, 4, seed=2), 1e-2, mode="nc2lmc")
-    pa = points(meshes, 0, 5000, seed=21)  # five 1,024-point chunks of the NC path
+    pa = points(meshes, 0, 5000, seed=21)  # chunks of at most 1,024 points: five or more per sweep
     ra = srv.submit(0, 0, pa, 3e-2, seed=5, mode="nc2lmc")
     mean_a, se_a, info_a = srv.wait(ra, timeout=300)
     check_accuracy(gpu, probs[0], pa, mean_a, se_a, info_a, 3e-2)
     assert info_a["residual_walks_per_point"] >= max(2, info_a["walks_per_point"] // 4)
-    assert info_a["ticks"] == 5 * info_a["sweeps"]
+    assert info_a["ticks"] >= 5 * info_a["sweeps"]
     mix = []
     for k, (mesh, prob, n, tgt, mode) in enumerate([(1, 1, 3000, 2e-2, "nc2lmc"), (0, 0, 800, 2e-2, "plain"),
                                                     (1, 1, 50, 1e-2, "plain"), (0, 0, 9, 1e-2, "nc2lmc")]):
@@ -136,6 +136,7 @@ def test_nc2lmc_requests_alone_equal_mix_and_unbiased(gpu, meshes):
     mean_b, se_b, info_b = srv.wait(rb, timeout=300)
     assert info_b["walks_per_point"] == info_a["walks_per_point"]
     assert info_b["residual_walks_per_point"] == info_a["residual_walks_per_point"]
+    assert info_b["ticks"] == info_a["ticks"]  # the same chunking alone and in the mix
     np.testing.assert_allclose(mean_b, mean_a, rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(se_b, se_a, rtol=1e-9, atol=1e-14)
     for rid, prob, p, tgt in mix:
