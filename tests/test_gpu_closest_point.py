@@ -181,3 +181,44 @@ def test_long_queries_handed_to_warp_finisher_stay_exact(gpu, masked):
     counted = bvh.query(centre[:1024], counted=True)
     work = counted["node_visits"] + counted["tri_tests"]
     assert np.mean(work > 320) > 0.1
+
+
+def test_degenerate_duplicate_and_single_triangle_meshes(gpu):
+    """A tetrahedron with a duplicated face and a zero-area sliver (ties on the
+    duplicate resolve to the lower id), and a one-triangle mesh; queries include
+    the vertices themselves.  Plain and counted launches equal the brute force."""
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0, 0]], np.float32)
+    t = np.array([[0, 2, 1], [0, 1, 3], [1, 2, 3], [0, 3, 2], [1, 2, 3], [0, 4, 1]], np.uint32)
+    pts = uniform_box(4000, 1.5, 11)
+    pts[:5] = v
+    for verts, tri in ((v, t), (v[:3], np.array([[0, 1, 2]], np.uint32))):
+        m = gpu.Mesh.from_arrays(verts, tri)
+        bf = oracle.bruteforce(verts, tri, pts)
+        for leaf in (1, 8):
+            bvh = gpu.Bvh(m, leaf, "sah")
+            for counted in (False, True):
+                r = bvh.query(pts, counted=counted)
+                assert_bitexact(r, bf)
+                assert not r["overflow"].any()
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 257, 4099])
+def test_ragged_query_counts(gpu, ref_bvh, golden_closest, n):
+    """Counts that fill no whole warp or block: every query still answered
+    exactly, and nothing past the end is written."""
+    from n2w._lib import call
+
+    pts = uniform_box(n, 1.2, 700 + n)
+    nodes, tris = ref_bvh.layout()
+    want = oracle.traverse4(nodes, tris, pts, seed=ref_bvh.seed_grid())
+    assert_bitexact(ref_bvh.query(pts), want)
+    # guard words after each output array stay untouched
+    dp = gpu.DeviceBuffer.from_array(pts)
+    guard = 0x7F7F7F7F
+    d2, cp, ids, ov = (gpu.DeviceBuffer.from_array(np.full(k * (n + 8), guard, np.uint32)) for k in (1, 3, 1, 1))
+    call("n2w_bvh_query_device", ref_bvh.handle, dp.ptr, n, d2.ptr, cp.ptr, ids.ptr, ov.ptr, 128, None)
+    for buf, k in ((d2, 1), (cp, 3), (ids, 1), (ov, 1)):
+        tail = buf.download(np.uint32)[k * n:]
+        assert (tail == guard).all()
+    assert np.array_equal(d2.download(np.float32)[:n].view(np.uint32), want["distance2"].view(np.uint32))
+    assert np.array_equal(ids.download(np.int32)[:n], want["triangle_id"])
