@@ -56,9 +56,15 @@ constexpr uint32_t kQueryBudget = 384;
 constexpr int kHandOff = 2;         // overflow-slot mark of a handed-off query
 constexpr int kFinishWarps = 4;     // warps per finisher block
 constexpr int kFinishStack = 2048;  // work-list entries per finisher warp (16 KiB)
+// Resident blocks per SM the traversal is compiled for (kMinBlocks).  Launches
+// of up to a few queries per lane run faster with 4 (up to 64 registers, no
+// spills) and larger ones with 5 (more warps to hide load latency): measured
+// 152.5 / 224.2 / 285.1 against 149.5 / 213.0 / 276.0 M queries/s at 131,072 /
+// 262,144 / 524,288 queries, equal at 1 M and 2 M, 391 against 405 at 4 M.
+constexpr int64_t kSmallLaunch = int64_t{1} << 21;
 
-template <bool kMasked, bool kCount>
-__global__ void __launch_bounds__(kQueryBlock, 5) closest_point_kernel(
+template <bool kMasked, bool kCount, int kMinBlocks>
+__global__ void __launch_bounds__(kQueryBlock, kMinBlocks) closest_point_kernel(
     const float4* __restrict__ nodes, const float4* __restrict__ tris, const dev::SeedGrid grid,
     const n2w_vec3* __restrict__ points, const uint8_t* __restrict__ active, int n,
     float* __restrict__ out_d2, n2w_vec3* __restrict__ out_cp, int* __restrict__ out_id,
@@ -344,12 +350,18 @@ void launch_closest_point(const n2w_bvh& bvh, const n2w_vec3* d_points, const ui
   if (d_nodes) {
     // the counting variant runs every query to completion in one lane, so its
     // counts are the single-lane traversal's (the algorithmic work)
-    launch(closest_point_kernel<false, true>, d_active, d_nodes, d_tris);
+    launch(closest_point_kernel<false, true, 5>, d_active, d_nodes, d_tris);
     N2W_CUDA(cudaGetLastError());
     return;
   }
-  if (d_active) launch(closest_point_kernel<true, false>, d_active, nullptr, nullptr);
-  else launch(closest_point_kernel<false, false>, nullptr, nullptr, nullptr);
+  const bool small = n < kSmallLaunch;
+  if (d_active) {
+    if (small) launch(closest_point_kernel<true, false, 4>, d_active, nullptr, nullptr);
+    else launch(closest_point_kernel<true, false, 5>, d_active, nullptr, nullptr);
+  } else {
+    if (small) launch(closest_point_kernel<false, false, 4>, nullptr, nullptr, nullptr);
+    else launch(closest_point_kernel<false, false, 5>, nullptr, nullptr, nullptr);
+  }
   N2W_CUDA(cudaGetLastError());
   const size_t smem = sizeof(int2) * kFinishWarps * kFinishStack;
   static thread_local int configured_device = -1;
