@@ -155,7 +155,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 //    warp returns to Phase A once `regen` lanes are waiting (or none is busy),
 //    so the walk updates run for many lanes at once and no lane waits for
 //    another lane's whole traversal.
-template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks>
+template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks, int kUnits = 1>
 __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(const __grid_constant__ WalkArgs a) {
   static_assert(!kBatch || (kOut == kOutStats && kWalk == N2W_WALK_PURE),
                 "batched launches run plain walks into per-point statistics");
@@ -419,11 +419,15 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
       const unsigned busy = __ballot_sync(0xffffffffu, querying);
       const unsigned waiting = __ballot_sync(0xffffffffu, !querying && alive);
       if (busy == 0 || __popc(waiting) >= a.regen) break;
-      // Two units of traversal per vote, written out twice: the votes and the
-      // exit test cost about as much as a unit, and a lane that finishes on
-      // the first unit waits at most one unit longer (headline slice, same
-      // box: one unit 1,031, two 1,070, three 1,040 M walk-steps/s; the same
-      // two units as an unrolled loop 1,054).
+      // kUnits = 2 runs two units of traversal per vote, written out twice: the
+      // votes and the exit test cost about as much as a unit, and a lane that
+      // finishes on the first unit waits at most one unit longer (headline
+      // slice, same box: one unit 1,031, two 1,070, three 1,040 M
+      // walk-steps/s; the two units as an unrolled loop 1,054).  Compiled in,
+      // the second unit slows walks whose steps carry several source samples
+      // (16 per ball: 29.4 ns per walk with one unit, 31.4 with the second
+      // unit present even when it is skipped), so they run the kUnits = 1
+      // kernel.
       if (querying) {
         bool ov = false;
         if (!dev::trav_step_fast(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
@@ -432,12 +436,14 @@ __global__ void __launch_bounds__(kWalkerMaxThreads, kMinBlocks) walker_kernel(c
           ++c_overflow;
         }
       }
-      if (querying) {
-        bool ov = false;
-        if (!dev::trav_step_fast(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
-        if (ov) {
-          w_overflow = true;
-          ++c_overflow;
+      if constexpr (kUnits == 2) {
+        if (querying) {
+          bool ov = false;
+          if (!dev::trav_step_fast(a.nodes, a.tris, x, hit, tv, stack, c_nodes, c_tris, ov)) querying = false;
+          if (ov) {
+            w_overflow = true;
+            ++c_overflow;
+          }
         }
       }
     }
@@ -593,9 +599,9 @@ __global__ void combine_kernel(const float* __restrict__ cache, const float* __r
 // ---- host side -----------------------------------------------------------
 namespace {
 
-template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks>
+template <int kOut, int kWalk, bool kBatch = false, int kMinBlocks = kWalkerMinBlocks, int kUnits = 1>
 void launch_walker(const WalkArgs& a, int block, int blocks_per_sm, cudaStream_t stream) {
-  auto kern = walker_kernel<kOut, kWalk, kBatch, kMinBlocks>;
+  auto kern = walker_kernel<kOut, kWalk, kBatch, kMinBlocks, kUnits>;
   int occ = 0;
   N2W_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, 0));
   if (occ < 1) occ = 1;
@@ -726,7 +732,11 @@ void run_walker(WalkArgs& a, int64_t point_count, int out_kind, int walk_mode, c
     N2W_CUDA(cudaGetLastError());
   }
   const int block = o.block_size > 0 ? o.block_size : kDefaultWalkerThreads;
-  if (out_kind == kOutStats) launch_walker<kOutStats, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
+  if (out_kind == kOutStats) {
+    // two traversal units per vote unless the steps carry several source samples
+    if (a.has_source && a.source_samples > 1) launch_walker<kOutStats, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
+    else launch_walker<kOutStats, N2W_WALK_PURE, false, kWalkerMinBlocks, 2>(a, block, o.blocks_per_sm, stream);
+  }
   else if (out_kind == kOutSamples) launch_walker<kOutSamples, N2W_WALK_PURE>(a, block, o.blocks_per_sm, stream);
   else if (walk_mode == N2W_WALK_PREFIX) launch_walker<kOutPrefix, N2W_WALK_PREFIX>(a, block, o.blocks_per_sm, stream);
   else launch_walker<kOutPrefix, N2W_WALK_RESIDUAL>(a, block, o.blocks_per_sm, stream);
