@@ -159,3 +159,57 @@ def test_data_parallel_gradients_equal_union_batch(tmp_path):
     p0, p1 = np.load(tmp_path / "p0.npy"), np.load(tmp_path / "p1.npy")
     np.testing.assert_array_equal(p0, p1)  # ranks stay identical
     np.testing.assert_allclose(p0, p, rtol=1e-10, atol=1e-13)
+
+
+def test_nccl_comm_id_handover(monkeypatch, tmp_path):
+    """NcclComm's host side for N > 1 ranks, with the library's NCCL calls
+    replaced by a stand-in (no GPU): rank 0's id reaches rank 1 through the
+    launch's file even when rank 1 starts first, both join with the same id,
+    the world size and their rank, the file is gone afterwards, and a rank
+    whose rank 0 never writes the id fails with a clear timeout."""
+    import ctypes as C
+    import threading
+
+    from n2w import _lib, shard
+
+    uid_bytes = bytes((7 * i + 3) & 0xFF for i in range(128))
+    joined = threading.Barrier(2, timeout=30)
+    seen = {}
+
+    def fake_call(name, *args):
+        if name == "n2w_comm_unique_id":
+            for i, b in enumerate(uid_bytes):
+                args[0][i] = b
+        elif name == "n2w_comm_create":
+            uid, world, rank, handle = args
+            seen[rank] = (bytes(uid), world)
+            joined.wait()  # like ncclCommInitRank: returns once every rank has joined
+            handle._obj.value = 1000 + rank
+        else:
+            raise AssertionError(f"unexpected call {name}")
+        return 0
+
+    monkeypatch.setattr(_lib, "call", fake_call)
+    comms, errors = {}, []
+
+    def join(rank):
+        try:
+            comms[rank] = shard.NcclComm(rank, 2, key="launch1", directory=str(tmp_path), timeout=30)
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=join, args=(r,)) for r in (1, 0)]  # rank 1 waits for the file
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(60)
+    try:
+        assert not errors, errors
+        assert seen[0] == seen[1] == (uid_bytes, 2)
+        assert (comms[0].rank, comms[1].rank, comms[0].world) == (0, 1, 2)
+        assert not (tmp_path / "n2w_nccl_launch1.id").exists()
+    finally:
+        for c in comms.values():
+            c.h = C.c_void_p()  # stand-in handles: nothing to destroy
+    with pytest.raises(TimeoutError, match="no NCCL id"):
+        shard.NcclComm(1, 2, key="no_rank0", directory=str(tmp_path), timeout=0.2)
