@@ -49,3 +49,15 @@ def test_reference_arm_loads_no_product_code(tmp_path, n2w):
     ref_sub = set(map(tuple, ref_pts.tolist()))
     assert all((tuple(p) in ref_sub) == bool(i) for p, i in zip(sub.tolist(), inside))
     assert d["points"] == 170364
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun only rank 0 runs the reference arm; the others exit 0
+    at once and print nothing."""
+    import os
+
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       capture_output=True, text=True, timeout=120, env=env, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
