@@ -437,8 +437,12 @@ int n2w_nc2lmc_estimate_ex(const n2w_bvh* bvh, const n2w_problem* problem, const
     N2W_REQUIRE(o->residual_walks == 0 || (residual.d_sum && residual.d_sum_sq && residual.d_count),
                 "null residual outputs");
     const int64_t wmax = std::max(o->coarse_walks, o->residual_walks);
+    // Auto batch: up to 2^24 samples per level launch (45 B of per-sample
+    // scratch each, ~0.75 GB), so a launch holds enough walks to fill the GPU
+    // (with 2^22, 1,024 coarse walks meant 4,096-point launches whose tails
+    // cost ~30 % of a block of the time-to-MSE run).
     const int64_t batch = std::min<int64_t>(
-        n, o->point_batch > 0 ? o->point_batch : std::max<int64_t>(1, (int64_t{1} << 22) / wmax));
+        n, o->point_batch > 0 ? o->point_batch : std::max<int64_t>(1, (int64_t{1} << 24) / wmax));
     const int64_t maxS = batch * std::max(o->coarse_walks, o->residual_walks);
     float* inp = stream_alloc<float>(3 * maxS, stream);
     float* bnd = stream_alloc<float>(maxS, stream);
